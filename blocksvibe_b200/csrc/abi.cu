@@ -1,0 +1,123 @@
+// extern "C" entry points of libb3dgpu.so (declared in include/b3dgpu.h): argument checks, dispatch on
+// the limb count, error reporting.  No device memory is allocated here.
+#include <cstdio>
+#include <string>
+
+#include "b3dgpu.h"
+#include "kernels.cuh"
+
+namespace b3d {
+#define B3D_DECL(L) extern template struct Launch<L>;
+B3D_FOR_EACH_L(B3D_DECL)
+#undef B3D_DECL
+}  // namespace b3d
+
+namespace {
+
+thread_local std::string g_error;
+
+int fail(int code, const std::string& what) {
+    g_error = what;
+    return code;
+}
+
+int cuda_status(int code, const char* fn) {
+    if (code == 0) return 0;
+    return fail(code, std::string(fn) + ": " + cudaGetErrorString((cudaError_t)code));
+}
+
+inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+#define B3D_DISPATCH(L, CALL)                                                  \
+    switch (L) {                                                               \
+        case 6: { using LX = b3d::Launch<6>; return CALL; }                     \
+        case 10: { using LX = b3d::Launch<10>; return CALL; }                   \
+        case 18: { using LX = b3d::Launch<18>; return CALL; }                   \
+        case 26: { using LX = b3d::Launch<26>; return CALL; }                   \
+        case 30: { using LX = b3d::Launch<30>; return CALL; }                   \
+        case 34: { using LX = b3d::Launch<34>; return CALL; }                   \
+        case 42: { using LX = b3d::Launch<42>; return CALL; }                   \
+        default: return fail(B3D_E_LIMBS, "no kernels compiled for L = " + std::to_string(L)); \
+    }
+
+bool nonneg(int64_t x) { return x >= 0; }
+
+}  // namespace
+
+extern "C" {
+
+int b3d_version(void) { return 100; }
+
+const char* b3d_last_error(void) { return g_error.c_str(); }
+
+int b3d_supported_limbs(int L) {
+    switch (L) {
+        case 6: case 10: case 18: case 26: case 30: case 34: case 42: return 1;
+        default: return 0;
+    }
+}
+
+int b3d_align(int L, const int32_t* m, const int64_t* e, int64_t plane, int64_t nbatch, int64_t R, int64_t K,
+              int64_t sb, int64_t sr, int64_t sk, const int64_t* bidx, int32_t* om, int64_t* oe, int64_t oplane,
+              int kmajor, void* stream) {
+    if (!nonneg(nbatch) || !nonneg(R) || !nonneg(K)) return fail(B3D_E_ARG, "b3d_align: negative size");
+    B3D_DISPATCH(L, cuda_status(LX::align(m, e, plane, nbatch, R, K, sb, sr, sk, bidx, om, oe, oplane, kmajor,
+                                         as_stream(stream)), "b3d_align"));
+}
+
+int b3d_gemm_aligned(int L, const int32_t* am, const int64_t* ae, int64_t aplane, const int32_t* bm,
+                     const int64_t* be, int64_t bplane, int64_t nbatch, int64_t M, int64_t N, int64_t K,
+                     int32_t* cm, int64_t* ce, int64_t cplane, void* stream) {
+    if (!nonneg(nbatch) || !nonneg(M) || !nonneg(N) || !nonneg(K)) return fail(B3D_E_ARG, "b3d_gemm_aligned: negative size");
+    B3D_DISPATCH(L, cuda_status(LX::gemm_aligned(am, ae, aplane, bm, be, bplane, nbatch, M, N, K, cm, ce, cplane,
+                                                as_stream(stream)), "b3d_gemm_aligned"));
+}
+
+int b3d_mul(int L, const int32_t* am, const int64_t* ae, int64_t aplane, const int64_t* aidx,
+            const int32_t* bm, const int64_t* be, int64_t bplane, const int64_t* bidx, int64_t n,
+            int32_t* cm, int64_t* ce, int64_t cplane, void* stream) {
+    if (!nonneg(n)) return fail(B3D_E_ARG, "b3d_mul: negative size");
+    B3D_DISPATCH(L, cuda_status(LX::mul(am, ae, aplane, aidx, bm, be, bplane, bidx, n, cm, ce, cplane,
+                                       as_stream(stream)), "b3d_mul"));
+}
+
+int b3d_add(int L, const int32_t* am, const int64_t* ae, int64_t aplane, const int64_t* aidx,
+            const int32_t* bm, const int64_t* be, int64_t bplane, const int64_t* bidx, int64_t n,
+            int32_t* cm, int64_t* ce, int64_t cplane, void* stream) {
+    if (!nonneg(n)) return fail(B3D_E_ARG, "b3d_add: negative size");
+    B3D_DISPATCH(L, cuda_status(LX::add(am, ae, aplane, aidx, bm, be, bplane, bidx, n, cm, ce, cplane,
+                                       as_stream(stream)), "b3d_add"));
+}
+
+int b3d_cauchy_level(int L, const int32_t* rm, const int64_t* re, int64_t rplane, const int32_t* hm,
+                     const int64_t* he, int64_t hplane, const b3d_level_tables* lv, int32_t* om, int64_t* oe,
+                     int64_t oplane, void* stream) {
+    if (!lv || lv->nb < 0 || lv->Mr < 0 || lv->Kc < 0 || lv->N < 0 || lv->m < 0 || lv->m >= lv->hlevels)
+        return fail(B3D_E_ARG, "b3d_cauchy_level: invalid level description");
+    b3d::CauchyLevel c{lv->m, lv->nb, lv->Mr, lv->Kc, lv->N, lv->hlevels, lv->Jh, lv->gsrc, lv->gj,
+                       lv->rowd, lv->nrow, lv->cold, lv->ncol, lv->col};
+    B3D_DISPATCH(L, cuda_status(LX::cauchy(rm, re, rplane, hm, he, hplane, c, om, oe, oplane, as_stream(stream)),
+                                "b3d_cauchy_level"));
+}
+
+int b3d_pole_level(int L, const int32_t* hm, const int64_t* he, int64_t hplane, const int32_t* Rm,
+                   const int64_t* Re, int64_t Rplane, const int32_t* Qm, const int64_t* Qe, int64_t Qplane,
+                   const int64_t* t_hrow, const int64_t* t_R, const int64_t* t_qL, const int64_t* t_slot,
+                   int64_t T, int64_t B, int S, int32_t* ym, int64_t* ye, int64_t yplane, int32_t* rm,
+                   int64_t* re, int64_t rplane, void* stream) {
+    if (!nonneg(T) || B < 1 || S < 1) return fail(B3D_E_ARG, "b3d_pole_level: invalid size");
+    B3D_DISPATCH(L, cuda_status(LX::pole(hm, he, hplane, Rm, Re, Rplane, Qm, Qe, Qplane, t_hrow, t_R, t_qL, t_slot,
+                                        T, B, S, ym, ye, yplane, rm, re, rplane, as_stream(stream)),
+                                "b3d_pole_level"));
+}
+
+int b3d_moments_level(int L, const int32_t* rm, const int64_t* re, int64_t rplane, const int32_t* pm,
+                      const int64_t* pe, int64_t pplane, const int64_t* q_slot, const int64_t* q_row,
+                      const int64_t* q_n, int64_t Q, int64_t N, int R1, int32_t* mm, int64_t* me, int64_t mplane,
+                      void* stream) {
+    if (!nonneg(Q) || !nonneg(N) || R1 < 1) return fail(B3D_E_ARG, "b3d_moments_level: invalid size");
+    B3D_DISPATCH(L, cuda_status(LX::moments(rm, re, rplane, pm, pe, pplane, q_slot, q_row, q_n, Q, N, R1, mm, me,
+                                           mplane, as_stream(stream)), "b3d_moments_level"));
+}
+
+}  // extern "C"

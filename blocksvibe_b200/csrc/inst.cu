@@ -1,0 +1,11 @@
+// One translation unit per limb count (compiled with -DB3D_L=<L>): instantiates the kernel launchers.
+#define B3D_DEFINE_LAUNCH
+#include "kernels.cuh"
+
+#ifndef B3D_L
+#error "compile with -DB3D_L=<limbs>"
+#endif
+
+namespace b3d {
+template struct Launch<B3D_L>;
+}

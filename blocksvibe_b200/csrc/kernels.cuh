@@ -1,0 +1,430 @@
+// CUDA-core kernels of the blocks_3d hot path (sm_100a): multiprecision alignment, products, batched
+// GEMM, the recursion's Cauchy and pole steps, and the derivative moments.  Every kernel is a template
+// over the limb count L; inst.cu instantiates the launchers once per L, abi.cu dispatches on L.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "mp.cuh"
+
+namespace b3d {
+
+// Per-level tables of the Cauchy step (device pointers; see Plan in the Python host code).
+struct CauchyLevel {
+    i64 m, nb, Mr, Kc, N;          // level, groups, rows per group, columns per group, S^2 B
+    i64 hlevels, Jh;               // h_inf layout: (2, hlevels, Jh, N)
+    const i64* gsrc;               // (nb) source parity of each group
+    const i64* gj;                 // (nb) h_inf spin index of each group
+    const i64* rowd;               // (nb, Mr) 2 D' per row
+    const i64* nrow;               // (nb) rows in use
+    const i64* cold;               // (nb, Kc) 2 D_i per column
+    const i64* ncol;               // (nb) columns in use
+    const i64* col;                // (nb, Kc) physical slot of each column
+};
+
+// ------------------------------------------------------------------------------------------------
+// Alignment: for each (batch b, row r) of a strided view X[b, r, k] (k < K), write the mantissas shifted
+// to the row's largest exponent E (truncated below it) and E.  Output element (b, r, k) goes to
+// (b * R + r) * K + k, or (b * K + k) * R + r when `kmajor` (columns of a GEMM's right operand).
+template <int L>
+__global__ void k_align(const int32_t* __restrict__ m, const i64* __restrict__ e, i64 plane,
+                        i64 nbatch, i64 R, i64 K, i64 sb, i64 sr, i64 sk, const i64* __restrict__ bidx,
+                        int32_t* __restrict__ om, i64* __restrict__ oe, i64 oplane, int kmajor) {
+    i64 t = blockIdx.x * (i64)blockDim.x + threadIdx.x;
+    if (t >= nbatch * R) return;
+    i64 b = t / R, r = t % R;
+    i64 base = (bidx ? bidx[b] : b) * sb + r * sr;
+    i64 E = EZ;
+    for (i64 k = 0; k < K; k++) {
+        i64 ek = e[base + k * sk];
+        if (ek > E && m[(L - 1) * plane + base + k * sk] != 0) E = ek;
+    }
+    oe[t] = E;
+    for (i64 k = 0; k < K; k++) {
+        i64 src = base + k * sk;
+        i64 dst = kmajor ? (b * K + k) * R + r : t * K + k;
+        u32 a[L];
+        bool neg = load_mag<L>(m, plane, src, a);
+        i64 ek = e[src];
+        u32 s[L];
+        if (E == EZ || is_zero(a) || ek == EZ || E - ek >= 32 * L) {
+            zero(s);
+            neg = false;
+        } else {
+            shr(a, (int)(E - ek), s);
+        }
+        store_signed<L>(om, oplane, dst, s, neg);
+    }
+}
+
+// Batched product of aligned operands: C[b, i, j] = sum_k A[b, i, k] B[b, k, j] with A rows and B
+// columns already aligned (k_align); exact accumulation, one rounding.  C is contiguous (b, i, j).
+template <int L>
+__global__ void k_gemm_aligned(const int32_t* __restrict__ am, const i64* __restrict__ ae, i64 aplane,
+                               const int32_t* __restrict__ bm, const i64* __restrict__ be, i64 bplane,
+                               i64 nbatch, i64 M, i64 N, i64 K, int32_t* __restrict__ cm, i64* __restrict__ ce,
+                               i64 cplane) {
+    i64 t = blockIdx.x * (i64)blockDim.x + threadIdx.x;
+    if (t >= nbatch * M * N) return;
+    i64 j = t % N, i = (t / N) % M, b = t / (M * N);
+    i64 Ea = ae[b * M + i], Eb = be[b * N + j];
+    constexpr int NW = 2 * L + 2;
+    u32 acc[NW];
+    zero(acc);
+    if (Ea != EZ && Eb != EZ) {
+        for (i64 k = 0; k < K; k++) {
+            u32 a[L], bb[L];
+            bool na = load_mag<L>(am, aplane, (b * M + i) * K + k, a);
+            if (is_zero(a)) continue;
+            bool nb = load_mag<L>(bm, bplane, (b * K + k) * N + j, bb);
+            if (is_zero(bb)) continue;
+            mac_signed<L, NW>(acc, a, bb, na != nb);
+        }
+    }
+    store_rounded<L, NW>(cm, ce, cplane, t, acc, (Ea == EZ || Eb == EZ) ? EZ : Ea + Eb);
+}
+
+// Elementwise C = A * B (exact product, one rounding); A and B indexed through optional gathers.
+template <int L>
+__global__ void k_mul(const int32_t* __restrict__ am, const i64* __restrict__ ae, i64 aplane, const i64* __restrict__ aidx,
+                      const int32_t* __restrict__ bm, const i64* __restrict__ be, i64 bplane, const i64* __restrict__ bidx,
+                      i64 n, int32_t* __restrict__ cm, i64* __restrict__ ce, i64 cplane) {
+    i64 t = blockIdx.x * (i64)blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    i64 ia = aidx ? aidx[t] : t, ib = bidx ? bidx[t] : t;
+    u32 a[L], b[L];
+    bool na = load_mag<L>(am, aplane, ia, a);
+    bool nb = load_mag<L>(bm, bplane, ib, b);
+    i64 ea = ae[ia], eb = be[ib];
+    constexpr int NW = 2 * L + 1;
+    u32 acc[NW];
+    zero(acc);
+    bool z = is_zero(a) || is_zero(b) || ea == EZ || eb == EZ;
+    if (!z) mac_signed<L, NW>(acc, a, b, na != nb);
+    store_rounded<L, NW>(cm, ce, cplane, t, acc, z ? EZ : ea + eb);
+}
+
+// Elementwise C = A + B (one rounding), optional gathers.
+template <int L>
+__global__ void k_add(const int32_t* __restrict__ am, const i64* __restrict__ ae, i64 aplane, const i64* __restrict__ aidx,
+                      const int32_t* __restrict__ bm, const i64* __restrict__ be, i64 bplane, const i64* __restrict__ bidx,
+                      i64 n, int32_t* __restrict__ cm, i64* __restrict__ ce, i64 cplane) {
+    i64 t = blockIdx.x * (i64)blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    i64 ia = aidx ? aidx[t] : t, ib = bidx ? bidx[t] : t;
+    u32 a[L], b[L], r[L];
+    bool na = load_mag<L>(am, aplane, ia, a);
+    bool nb = load_mag<L>(bm, bplane, ib, b);
+    bool nr;
+    i64 er;
+    add_norm<L>(a, na, ae[ia], b, nb, be[ib], r, &nr, &er);
+    store_signed<L>(cm, cplane, t, r, nr);
+    ce[t] = er;
+}
+
+// ------------------------------------------------------------------------------------------------
+// Cauchy step of recursion level m, fused with the h_inf term:
+//   H[g, r, n] = hinf[gsrc[g], m, gj[g], n] + sum_{i < ncol[g]} 2 / (rowd[g, r] - cold[g, i]) res[col[g, i], n]
+// (terms with a vanishing difference are skipped; rows r >= nrow[g] are padding and written as zero).
+// The residues of a column (g, n) are aligned to their largest exponent, each term 2 x / d is formed
+// exactly up to 32 guard bits (one-limb division), the sum is exact, rounded once, then h_inf is added
+// with one more rounding.
+template <int L>
+__global__ void k_cauchy(const int32_t* __restrict__ rm, const i64* __restrict__ re, i64 rplane,
+                         const int32_t* __restrict__ hm, const i64* __restrict__ he, i64 hplane,
+                         CauchyLevel lv, int32_t* __restrict__ om, i64* __restrict__ oe, i64 oplane) {
+    i64 t = blockIdx.x * (i64)blockDim.x + threadIdx.x;
+    i64 N = lv.N;
+    if (t >= lv.nb * lv.Mr * N) return;
+    i64 n = t % N, r = (t / N) % lv.Mr, g = t / (N * lv.Mr);
+    if (r >= lv.nrow[g]) {
+        u32 z[L];
+        zero(z);
+        store_signed<L>(om, oplane, t, z, false);
+        oe[t] = EZ;
+        return;
+    }
+    i64 hidx = ((lv.gsrc[g] * lv.hlevels + lv.m) * lv.Jh + lv.gj[g]) * N + n;
+    u32 h[L];
+    bool nh = load_mag<L>(hm, hplane, hidx, h);
+    i64 eh = he[hidx];
+    i64 ncol = lv.ncol[g];
+    const i64* col = lv.col + g * lv.Kc;
+    const i64* cold = lv.cold + g * lv.Kc;
+    i64 D = lv.rowd[g * lv.Mr + r];
+    i64 E = EZ;
+    for (i64 i = 0; i < ncol; i++) {
+        i64 ix = col[i] * N + n;
+        i64 ei = re[ix];
+        if (ei > E && rm[(L - 1) * rplane + ix] != 0) E = ei;
+    }
+    u32 s[L];
+    bool ns = false;
+    i64 es = EZ;
+    if (E != EZ) {
+        constexpr int NW = L + 3;
+        u32 acc[NW];
+        zero(acc);
+        for (i64 i = 0; i < ncol; i++) {
+            i64 d = D - cold[i];
+            if (d == 0) continue;
+            i64 ix = col[i] * N + n;
+            u32 a[L];
+            bool na = load_mag<L>(rm, rplane, ix, a);
+            i64 ei = re[ix];
+            if (is_zero(a) || ei == EZ || E - ei >= 32 * L) continue;
+            u32 x[L];
+            shr(a, (int)(E - ei), x);
+            if (d < 0) { na = !na; d = -d; }
+            u32 q[L + 1];
+            div_small<L>(x, (u32)d, q);
+            add_signed(acc, q, na);
+        }
+        bool neg = (acc[NW - 1] >> 31) != 0;
+        if (neg) negate(acc);
+        if (round_mag<L>(acc, E - 31, s, &es)) ns = neg;   // value = acc 2^(E - 32) x 2
+    } else {
+        zero(s);
+    }
+    u32 out[L];
+    bool no;
+    i64 eo;
+    add_norm<L>(s, ns, es, h, nh, eh, out, &no, &eo);
+    store_signed<L>(om, oplane, t, out, no);
+    oe[t] = eo;
+}
+
+// ------------------------------------------------------------------------------------------------
+// Pole step, stage 1: Y[t, a, b0, k] = sum_b R[b0, b] H[t_hrow[t], a, b, k]  (R = Rtab[t_R[t]] aligned
+// per row; H aligned per column (a, k) over b here).  Y: (T, S, S, B) contiguous.
+template <int L>
+__global__ void k_pole1(const int32_t* __restrict__ hm, const i64* __restrict__ he, i64 hplane,
+                        const int32_t* __restrict__ Rm, const i64* __restrict__ Re, i64 Rplane,
+                        const i64* __restrict__ t_hrow, const i64* __restrict__ t_R, i64 T, i64 B, int S,
+                        int32_t* __restrict__ ym, i64* __restrict__ ye, i64 yplane) {
+    i64 idx = blockIdx.x * (i64)blockDim.x + threadIdx.x;
+    if (idx >= T * S * S * B) return;
+    i64 k = idx % B, b0 = (idx / B) % S, a = (idx / (B * S)) % S, t = idx / (B * S * S);
+    i64 hrow = t_hrow[t], rk = t_R[t];
+    i64 hb = hrow * S * S * B + a * S * B + k;          // H[hrow, a, b, k] at hb + b * B
+    i64 E = EZ;
+    for (int b = 0; b < S; b++) {
+        i64 ix = hb + b * B;
+        i64 eb = he[ix];
+        if (eb > E && hm[(L - 1) * hplane + ix] != 0) E = eb;
+    }
+    i64 Er = Re[rk * S + b0];
+    constexpr int NW = 2 * L + 2;
+    u32 acc[NW];
+    zero(acc);
+    if (E != EZ && Er != EZ) {
+#pragma unroll 1
+        for (int b = 0; b < S; b++) {
+            u32 x[L], y[L], r[L];
+            bool nr = load_mag<L>(Rm, Rplane, (rk * S + b0) * S + b, r);
+            if (is_zero(r)) continue;
+            i64 ix = hb + b * B;
+            bool nx = load_mag<L>(hm, hplane, ix, x);
+            i64 ex = he[ix];
+            if (is_zero(x) || ex == EZ || E - ex >= 32 * L) continue;
+            shr(x, (int)(E - ex), y);
+            mac_signed<L, NW>(acc, r, y, nr != nx);
+        }
+    }
+    store_rounded<L, NW>(ym, ye, yplane, idx, acc, (E == EZ || Er == EZ) ? EZ : E + Er);
+}
+
+// Pole step, stage 2: res[t_slot[t], a0, b0, k] = sum_a QL[a0, a] Y[t, a, b0, k]  (QL = QLtab[t_qL[t]]
+// aligned per row; Y aligned per column (b0, k) over a here).
+template <int L>
+__global__ void k_pole2(const int32_t* __restrict__ ym, const i64* __restrict__ ye, i64 yplane,
+                        const int32_t* __restrict__ Qm, const i64* __restrict__ Qe, i64 Qplane,
+                        const i64* __restrict__ t_qL, const i64* __restrict__ t_slot, i64 T, i64 B, int S,
+                        int32_t* __restrict__ rm, i64* __restrict__ re, i64 rplane) {
+    i64 idx = blockIdx.x * (i64)blockDim.x + threadIdx.x;
+    if (idx >= T * S * S * B) return;
+    i64 k = idx % B, b0 = (idx / B) % S, a0 = (idx / (B * S)) % S, t = idx / (B * S * S);
+    i64 qk = t_qL[t];
+    i64 yb = t * S * S * B + b0 * B + k;                // Y[t, a, b0, k] at yb + a * S * B
+    i64 E = EZ;
+    for (int a = 0; a < S; a++) {
+        i64 ix = yb + a * S * B;
+        i64 ea = ye[ix];
+        if (ea > E && ym[(L - 1) * yplane + ix] != 0) E = ea;
+    }
+    i64 Eq = Qe[qk * S + a0];
+    constexpr int NW = 2 * L + 2;
+    u32 acc[NW];
+    zero(acc);
+    if (E != EZ && Eq != EZ) {
+#pragma unroll 1
+        for (int a = 0; a < S; a++) {
+            u32 x[L], y[L], q[L];
+            bool nq = load_mag<L>(Qm, Qplane, (qk * S + a0) * S + a, q);
+            if (is_zero(q)) continue;
+            i64 ix = yb + a * S * B;
+            bool nx = load_mag<L>(ym, yplane, ix, x);
+            i64 ex = ye[ix];
+            if (is_zero(x) || ex == EZ || E - ex >= 32 * L) continue;
+            shr(x, (int)(E - ex), y);
+            mac_signed<L, NW>(acc, q, y, nq != nx);
+        }
+    }
+    i64 out = t_slot[t] * S * S * B + (a0 * S + b0) * B + k;
+    store_rounded<L, NW>(rm, re, rplane, out, acc, (E == EZ || Eq == EZ) ? EZ : E + Eq);
+}
+
+// ------------------------------------------------------------------------------------------------
+// Derivative moments of one recursion level: for each moment entry q (slot, row, n) and column c,
+//   y = res[slot, c] * rc^n,   mom[row, kk, c] += n^kk y   (kk <= R)
+// mom layout (rows, R + 1, N).  n^kk y is formed exactly from the previous power (one-limb product)
+// and rounded before each addition.
+template <int L>
+__global__ void k_moments(const int32_t* __restrict__ rm, const i64* __restrict__ re, i64 rplane,
+                          const int32_t* __restrict__ pm, const i64* __restrict__ pe, i64 pplane,
+                          const i64* __restrict__ q_slot, const i64* __restrict__ q_row, const i64* __restrict__ q_n,
+                          i64 Q, i64 N, int R1, int32_t* __restrict__ mm, i64* __restrict__ me, i64 mplane) {
+    i64 t = blockIdx.x * (i64)blockDim.x + threadIdx.x;
+    if (t >= Q * N) return;
+    i64 c = t % N, q = t / N;
+    i64 ix = q_slot[q] * N + c, nn = q_n[q];
+    u32 x[L], p[L];
+    bool nx = load_mag<L>(rm, rplane, ix, x);
+    bool np = load_mag<L>(pm, pplane, nn, p);
+    i64 ex = re[ix], ep = pe[nn];
+    if (is_zero(x) || is_zero(p) || ex == EZ || ep == EZ) return;
+    constexpr int NW = 2 * L + 1;
+    u32 acc[NW];
+    zero(acc);
+    mac_signed<L, NW>(acc, x, p, false);
+    u32 y[L];
+    i64 ey;
+    round_mag<L>(acc, ex + ep, y, &ey);
+    bool ny = nx != np;
+    i64 row = q_row[q];
+    for (int kk = 0; kk < R1; kk++) {
+        i64 o = (row * R1 + kk) * N + c;
+        u32 v[L], s[L];
+        bool nv = load_mag<L>(mm, mplane, o, v);
+        bool ns;
+        i64 es;
+        add_norm<L>(v, nv, me[o], y, ny, ey, s, &ns, &es);
+        store_signed<L>(mm, mplane, o, s, ns);
+        me[o] = es;
+        if (kk + 1 < R1) {                             // y *= n (exact, then rounded)
+            u32 w[L + 1];
+            u64 carry = 0;
+#pragma unroll
+            for (int k = 0; k < L; k++) {
+                u64 v2 = (u64)y[k] * (u64)nn + carry;
+                w[k] = (u32)v2;
+                carry = v2 >> 32;
+            }
+            w[L] = (u32)carry;
+            if (nn == 0) {                             // 0^kk = 0 for kk >= 1
+                ey = EZ;
+                zero(y);
+            } else {
+                round_mag<L>(w, ey, y, &ey);
+            }
+        }
+    }
+}
+
+// ------------------------------------------------------------------------------------------------
+// Host-side launchers, one instantiation per limb count (inst.cu).  Each returns a cudaError_t code.
+inline unsigned grid_for(i64 n, int th) { return (unsigned)((n + th - 1) / th); }
+
+template <int L>
+struct Launch {
+    static int align(const int32_t* m, const i64* e, i64 plane, i64 nbatch, i64 R, i64 K, i64 sb, i64 sr, i64 sk,
+                     const i64* bidx, int32_t* om, i64* oe, i64 oplane, int kmajor, cudaStream_t st);
+    static int gemm_aligned(const int32_t* am, const i64* ae, i64 aplane, const int32_t* bm, const i64* be, i64 bplane,
+                            i64 nbatch, i64 M, i64 N, i64 K, int32_t* cm, i64* ce, i64 cplane, cudaStream_t st);
+    static int mul(const int32_t* am, const i64* ae, i64 aplane, const i64* aidx, const int32_t* bm, const i64* be,
+                   i64 bplane, const i64* bidx, i64 n, int32_t* cm, i64* ce, i64 cplane, cudaStream_t st);
+    static int add(const int32_t* am, const i64* ae, i64 aplane, const i64* aidx, const int32_t* bm, const i64* be,
+                   i64 bplane, const i64* bidx, i64 n, int32_t* cm, i64* ce, i64 cplane, cudaStream_t st);
+    static int cauchy(const int32_t* rm, const i64* re, i64 rplane, const int32_t* hm, const i64* he, i64 hplane,
+                      const CauchyLevel& lv, int32_t* om, i64* oe, i64 oplane, cudaStream_t st);
+    static int pole(const int32_t* hm, const i64* he, i64 hplane, const int32_t* Rm, const i64* Re, i64 Rplane,
+                    const int32_t* Qm, const i64* Qe, i64 Qplane, const i64* t_hrow, const i64* t_R, const i64* t_qL,
+                    const i64* t_slot, i64 T, i64 B, int S, int32_t* ym, i64* ye, i64 yplane,
+                    int32_t* rm, i64* re, i64 rplane, cudaStream_t st);
+    static int moments(const int32_t* rm, const i64* re, i64 rplane, const int32_t* pm, const i64* pe, i64 pplane,
+                       const i64* q_slot, const i64* q_row, const i64* q_n, i64 Q, i64 N, int R1,
+                       int32_t* mm, i64* me, i64 mplane, cudaStream_t st);
+};
+
+#ifdef B3D_DEFINE_LAUNCH
+constexpr int kThreads = 128;
+
+template <int L>
+int Launch<L>::align(const int32_t* m, const i64* e, i64 plane, i64 nbatch, i64 R, i64 K, i64 sb, i64 sr, i64 sk,
+                     const i64* bidx, int32_t* om, i64* oe, i64 oplane, int kmajor, cudaStream_t st) {
+    i64 n = nbatch * R;
+    if (n == 0) return 0;
+    k_align<L><<<grid_for(n, kThreads), kThreads, 0, st>>>(m, e, plane, nbatch, R, K, sb, sr, sk, bidx, om, oe, oplane, kmajor);
+    return (int)cudaGetLastError();
+}
+
+template <int L>
+int Launch<L>::gemm_aligned(const int32_t* am, const i64* ae, i64 aplane, const int32_t* bm, const i64* be, i64 bplane,
+                            i64 nbatch, i64 M, i64 N, i64 K, int32_t* cm, i64* ce, i64 cplane, cudaStream_t st) {
+    i64 n = nbatch * M * N;
+    if (n == 0) return 0;
+    k_gemm_aligned<L><<<grid_for(n, kThreads), kThreads, 0, st>>>(am, ae, aplane, bm, be, bplane, nbatch, M, N, K, cm, ce, cplane);
+    return (int)cudaGetLastError();
+}
+
+template <int L>
+int Launch<L>::mul(const int32_t* am, const i64* ae, i64 aplane, const i64* aidx, const int32_t* bm, const i64* be,
+                   i64 bplane, const i64* bidx, i64 n, int32_t* cm, i64* ce, i64 cplane, cudaStream_t st) {
+    if (n == 0) return 0;
+    k_mul<L><<<grid_for(n, kThreads), kThreads, 0, st>>>(am, ae, aplane, aidx, bm, be, bplane, bidx, n, cm, ce, cplane);
+    return (int)cudaGetLastError();
+}
+
+template <int L>
+int Launch<L>::add(const int32_t* am, const i64* ae, i64 aplane, const i64* aidx, const int32_t* bm, const i64* be,
+                   i64 bplane, const i64* bidx, i64 n, int32_t* cm, i64* ce, i64 cplane, cudaStream_t st) {
+    if (n == 0) return 0;
+    k_add<L><<<grid_for(n, kThreads), kThreads, 0, st>>>(am, ae, aplane, aidx, bm, be, bplane, bidx, n, cm, ce, cplane);
+    return (int)cudaGetLastError();
+}
+
+template <int L>
+int Launch<L>::cauchy(const int32_t* rm, const i64* re, i64 rplane, const int32_t* hm, const i64* he, i64 hplane,
+                      const CauchyLevel& lv, int32_t* om, i64* oe, i64 oplane, cudaStream_t st) {
+    i64 n = lv.nb * lv.Mr * lv.N;
+    if (n == 0) return 0;
+    k_cauchy<L><<<grid_for(n, kThreads), kThreads, 0, st>>>(rm, re, rplane, hm, he, hplane, lv, om, oe, oplane);
+    return (int)cudaGetLastError();
+}
+
+template <int L>
+int Launch<L>::pole(const int32_t* hm, const i64* he, i64 hplane, const int32_t* Rm, const i64* Re, i64 Rplane,
+                    const int32_t* Qm, const i64* Qe, i64 Qplane, const i64* t_hrow, const i64* t_R, const i64* t_qL,
+                    const i64* t_slot, i64 T, i64 B, int S, int32_t* ym, i64* ye, i64 yplane,
+                    int32_t* rm, i64* re, i64 rplane, cudaStream_t st) {
+    i64 n = T * S * S * B;
+    if (n == 0) return 0;
+    k_pole1<L><<<grid_for(n, kThreads), kThreads, 0, st>>>(hm, he, hplane, Rm, Re, Rplane, t_hrow, t_R, T, B, S, ym, ye, yplane);
+    k_pole2<L><<<grid_for(n, kThreads), kThreads, 0, st>>>(ym, ye, yplane, Qm, Qe, Qplane, t_qL, t_slot, T, B, S, rm, re, rplane);
+    return (int)cudaGetLastError();
+}
+
+template <int L>
+int Launch<L>::moments(const int32_t* rm, const i64* re, i64 rplane, const int32_t* pm, const i64* pe, i64 pplane,
+                       const i64* q_slot, const i64* q_row, const i64* q_n, i64 Q, i64 N, int R1,
+                       int32_t* mm, i64* me, i64 mplane, cudaStream_t st) {
+    i64 n = Q * N;
+    if (n == 0) return 0;
+    k_moments<L><<<grid_for(n, kThreads), kThreads, 0, st>>>(rm, re, rplane, pm, pe, pplane, q_slot, q_row, q_n, Q, N, R1, mm, me, mplane);
+    return (int)cudaGetLastError();
+}
+#endif
+
+// limb counts with compiled kernels: 2 ceil(prec / 64) + 2 for precisions 128 ... 1280 bits, plus 6
+#define B3D_FOR_EACH_L(X) X(6) X(10) X(18) X(26) X(30) X(34) X(42)
+
+}  // namespace b3d

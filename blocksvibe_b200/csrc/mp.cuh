@@ -1,0 +1,290 @@
+// Multiprecision primitives on register arrays (sm_100a CUDA cores).
+//
+// Number format ("MPF", the layout of the reference's sdpvibe.mpf as used by blocksvibe): a value is
+// m * 2^e with m a signed integer of L 32-bit limbs (two's complement, limb 0 least significant) and e an
+// int64 exponent.  Normalised numbers have |m| of exactly NB = 32 L - 2 bits; zero is m = 0, e = EZ.
+// Arrays store limb planes: limb k of element i at m[k * plane + i].
+//
+// Everything here works on fixed-size register arrays (sizes are template parameters, all indexing is
+// static), so the compiler keeps the limbs in registers: variable shifts use a log-depth barrel shifter
+// instead of a runtime word index.
+#pragma once
+#include <cstdint>
+
+namespace b3d {
+
+typedef uint32_t u32;
+typedef uint64_t u64;
+typedef int64_t i64;
+
+constexpr i64 EZ = -(i64(1) << 60);       // exponent of zero
+constexpr int nb_bits(int L) { return 32 * L - 2; }
+
+#ifdef __CUDACC__
+#define B3D_HD __host__ __device__ __forceinline__
+#else
+#define B3D_HD inline
+#endif
+
+B3D_HD int clz32(u32 x) {
+#ifdef __CUDA_ARCH__
+    return __clz(x);
+#else
+    return x ? __builtin_clz(x) : 32;
+#endif
+}
+
+B3D_HD u32 umulhi32(u32 a, u32 b) {
+#ifdef __CUDA_ARCH__
+    return __umulhi(a, b);
+#else
+    return (u32)(((u64)a * b) >> 32);
+#endif
+}
+
+// (c2:c1:c0) += a * b  (96-bit column accumulator of product scanning)
+B3D_HD void mac96(u32& c0, u32& c1, u32& c2, u32 a, u32 b) {
+#ifdef __CUDA_ARCH__
+    asm("mad.lo.cc.u32 %0, %3, %4, %0;\n\t"
+        "madc.hi.cc.u32 %1, %3, %4, %1;\n\t"
+        "addc.u32 %2, %2, 0;"
+        : "+r"(c0), "+r"(c1), "+r"(c2) : "r"(a), "r"(b));
+#else
+    u64 p = (u64)a * b;
+    u64 lo = (u64)c0 + (u32)p;
+    u64 hi = (u64)c1 + (p >> 32) + (lo >> 32);
+    c0 = (u32)lo; c1 = (u32)hi; c2 += (u32)(hi >> 32);
+#endif
+}
+
+template <int N> B3D_HD void zero(u32 (&a)[N]) {
+#pragma unroll
+    for (int k = 0; k < N; k++) a[k] = 0;
+}
+
+// two's complement negation in place
+template <int N> B3D_HD void negate(u32 (&a)[N]) {
+    u32 c = 1;
+#pragma unroll
+    for (int k = 0; k < N; k++) {
+        u32 v = ~a[k] + c;
+        c = (c && v == 0) ? 1u : 0u;
+        a[k] = v;
+    }
+}
+
+template <int N> B3D_HD bool is_zero(const u32 (&a)[N]) {
+    u32 o = 0;
+#pragma unroll
+    for (int k = 0; k < N; k++) o |= a[k];
+    return o == 0;
+}
+
+// bit length of an unsigned array (0 for zero)
+template <int N> B3D_HD int bitlen(const u32 (&a)[N]) {
+    int bl = 0;
+#pragma unroll
+    for (int k = 0; k < N; k++)
+        if (a[k]) bl = 32 * k + 32 - clz32(a[k]);
+    return bl;
+}
+
+// out = floor(in / 2^sh), low NO limbs (sh >= 0; any size)
+template <int NI, int NO> B3D_HD void shr(const u32 (&in)[NI], int sh, u32 (&out)[NO]) {
+    constexpr int NT = (NI > NO + 1 ? NI : NO + 1);
+    u32 t[NT];
+#pragma unroll
+    for (int k = 0; k < NT; k++) t[k] = k < NI ? in[k] : 0u;
+    int w = sh >> 5, b = sh & 31;
+    if (w >= NI) { zero(out); return; }
+#pragma unroll
+    for (int s = 1; s < NT; s <<= 1) {
+        if (w & s) {
+#pragma unroll
+            for (int k = 0; k < NT; k++) t[k] = (k + s < NT) ? t[k + s] : 0u;
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < NO; k++) {
+        u32 lo = t[k], hi = (k + 1 < NT) ? t[k + 1] : 0u;
+        out[k] = b ? ((lo >> b) | (hi << (32 - b))) : lo;
+    }
+}
+
+// out = (in * 2^sh) mod 2^(32 NO)  (sh >= 0)
+template <int NI, int NO> B3D_HD void shl(const u32 (&in)[NI], int sh, u32 (&out)[NO]) {
+    u32 t[NO];
+#pragma unroll
+    for (int k = 0; k < NO; k++) t[k] = k < NI ? in[k] : 0u;
+    int w = sh >> 5, b = sh & 31;
+    if (w >= NO) { zero(out); return; }
+#pragma unroll
+    for (int s = 1; s < NO; s <<= 1) {
+        if (w & s) {
+#pragma unroll
+            for (int k = NO - 1; k >= 0; k--) t[k] = (k - s >= 0) ? t[k - s] : 0u;
+        }
+    }
+#pragma unroll
+    for (int k = NO - 1; k >= 0; k--) {
+        u32 hi = t[k], lo = (k > 0) ? t[k - 1] : 0u;
+        out[k] = b ? ((hi << b) | (lo >> (32 - b))) : hi;
+    }
+}
+
+// load one element of a limb-plane array as sign + magnitude
+template <int L> B3D_HD bool load_mag(const int32_t* m, i64 plane, i64 i, u32 (&a)[L]) {
+#pragma unroll
+    for (int k = 0; k < L; k++) a[k] = (u32)m[k * plane + i];
+    bool neg = (a[L - 1] >> 31) != 0;
+    if (neg) negate(a);
+    return neg;
+}
+
+template <int L> B3D_HD void store_signed(int32_t* m, i64 plane, i64 i, const u32 (&a)[L], bool neg) {
+    u32 t[L];
+#pragma unroll
+    for (int k = 0; k < L; k++) t[k] = a[k];
+    if (neg) negate(t);
+#pragma unroll
+    for (int k = 0; k < L; k++) m[k * plane + i] = (int32_t)t[k];
+}
+
+// Round an unsigned magnitude w (NW limbs, value w * 2^ein) to NB = 32 L - 2 bits, half away from zero.
+// Returns false for zero.  r: L-limb magnitude, *eout: exponent.
+template <int L, int NW> B3D_HD bool round_mag(const u32 (&w)[NW], i64 ein, u32 (&r)[L], i64* eout) {
+    constexpr int NB = nb_bits(L);
+    int bl = bitlen(w);
+    if (bl == 0) { zero(r); *eout = EZ; return false; }
+    int s = bl - NB;
+    if (s <= 0) {
+        shl(w, -s, r);
+        *eout = ein + s;
+        return true;
+    }
+    u32 t[L + 1];
+    shr(w, s - 1, t);                      // keeps the rounding bit in bit 0
+    u32 c = t[0] & 1u;
+#pragma unroll
+    for (int k = 0; k < L; k++) {
+        u32 v = (t[k] >> 1) | (t[k + 1] << 31);
+        u32 sum = v + c;
+        c = (c && sum == 0) ? 1u : 0u;
+        r[k] = sum;
+    }
+    // a carry out of bit NB - 1 makes the magnitude 2^NB: renormalise
+    if ((r[L - 1] >> (NB - 32 * (L - 1))) != 0) {
+        u32 q[L];
+        shr(r, 1, q);
+#pragma unroll
+        for (int k = 0; k < L; k++) r[k] = q[k];
+        s += 1;
+    }
+    *eout = ein + s;
+    return true;
+}
+
+// Round a two's complement accumulator (NW limbs, value acc * 2^ein) and store it normalised.
+template <int L, int NW> B3D_HD void store_rounded(int32_t* m, i64* e, i64 plane, i64 i, const u32 (&acc)[NW], i64 ein) {
+    u32 w[NW];
+#pragma unroll
+    for (int k = 0; k < NW; k++) w[k] = acc[k];
+    bool neg = (w[NW - 1] >> 31) != 0;
+    if (neg) negate(w);
+    u32 r[L];
+    i64 er;
+    if (!round_mag<L>(w, ein, r, &er)) neg = false;
+    store_signed<L>(m, plane, i, r, neg);
+    e[i] = er;
+}
+
+// acc (two's complement, NW >= 2 L + 1 limbs) += sgn * a * b, a and b magnitudes of L limbs
+// (product scanning: one 96-bit column at a time, merged into acc with a signed running carry)
+template <int L, int NW> B3D_HD void mac_signed(u32 (&acc)[NW], const u32 (&a)[L], const u32 (&b)[L], bool negative) {
+    u32 c0 = 0, c1 = 0, c2 = 0;
+    i64 rc = 0;
+#pragma unroll
+    for (int col = 0; col < 2 * L; col++) {
+#pragma unroll
+        for (int x = 0; x < L; x++) {
+            int y = col - x;
+            if (y >= 0 && y < L) mac96(c0, c1, c2, a[x], b[y]);
+        }
+        i64 r = (i64)acc[col] + (negative ? -(i64)c0 : (i64)c0) + rc;
+        acc[col] = (u32)r;
+        rc = r >> 32;
+        c0 = c1; c1 = c2; c2 = 0;
+    }
+#pragma unroll
+    for (int k = 2 * L; k < NW; k++) {
+        i64 r = (i64)acc[k] + rc;
+        acc[k] = (u32)r;
+        rc = r >> 32;
+    }
+}
+
+// acc (two's complement) += sgn * q, q an unsigned magnitude of NQ limbs (NQ <= NW)
+template <int NQ, int NW> B3D_HD void add_signed(u32 (&acc)[NW], const u32 (&q)[NQ], bool negative) {
+    i64 rc = 0;
+#pragma unroll
+    for (int k = 0; k < NW; k++) {
+        i64 v = k < NQ ? (i64)q[k] : 0;
+        i64 r = (i64)acc[k] + (negative ? -v : v) + rc;
+        acc[k] = (u32)r;
+        rc = r >> 32;
+    }
+}
+
+// floor(a * 2^32 / d) for an L-limb magnitude a and 0 < d < 2^16; L + 1 limbs
+template <int L> B3D_HD void div_small(const u32 (&a)[L], u32 d, u32 (&q)[L + 1]) {
+    u32 inv = 0xFFFFFFFFu / d;
+    u32 rem = 0;
+#pragma unroll
+    for (int k = L; k >= 0; k--) {
+        u32 limb = k > 0 ? a[k - 1] : 0u;
+        u32 out = 0;
+#pragma unroll
+        for (int h = 1; h >= 0; h--) {           // two 16-bit digits per limb: cur < d 2^16 <= 2^32
+            u32 cur = (rem << 16) | ((limb >> (16 * h)) & 0xFFFFu);
+            u32 qq = umulhi32(cur, inv);
+            u32 rr = cur - qq * d;
+            while (rr >= d) { qq++; rr -= d; }
+            out = (out << 16) | qq;
+            rem = rr;
+        }
+        q[k] = out;
+    }
+}
+
+// r = a + b for normalised operands (one rounding); returns the sign of r through *neg
+template <int L> B3D_HD void add_norm(const u32 (&a)[L], bool na, i64 ea, const u32 (&b)[L], bool nb, i64 eb,
+                                      u32 (&r)[L], bool* nr, i64* er) {
+    bool za = is_zero(a) || ea == EZ, zb = is_zero(b) || eb == EZ;
+    if (za && zb) { zero(r); *nr = false; *er = EZ; return; }
+    if (za) {
+#pragma unroll
+        for (int k = 0; k < L; k++) r[k] = b[k];
+        *nr = nb; *er = eb; return;
+    }
+    if (zb) {
+#pragma unroll
+        for (int k = 0; k < L; k++) r[k] = a[k];
+        *nr = na; *er = ea; return;
+    }
+    i64 top = ea > eb ? ea : eb;
+    i64 T = top - 32;                        // common grid: 32 guard bits below the larger operand's ulp
+    u32 acc[L + 2];
+    zero(acc);
+    u32 t[L + 2];
+    i64 da = ea - T, db = eb - T;            // >= 0 means a left shift
+    if (da >= 0) shl(a, (int)da, t); else shr(a, (int)(-da > 64 * L ? 64 * L : -da), t);
+    add_signed(acc, t, na);
+    if (db >= 0) shl(b, (int)db, t); else shr(b, (int)(-db > 64 * L ? 64 * L : -db), t);
+    add_signed(acc, t, nb);
+    bool neg = (acc[L + 1] >> 31) != 0;
+    if (neg) negate(acc);
+    if (!round_mag<L>(acc, T, r, er)) { *nr = false; return; }
+    *nr = neg;
+}
+
+}  // namespace b3d

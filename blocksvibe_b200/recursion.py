@@ -1,0 +1,116 @@
+"""Batched radial recursion of blocks_3d on one B200: the host half of the reference's
+``recursion_gpu.Recursion`` (``blocksvibe/recursion_gpu.py:379-514``), same constructor and ``run``
+contract.
+
+Per level m (a ``Plan`` level): one kernel for the Cauchy step fused with the h_inf term
+(``b3d_cauchy_level``), one pair of kernels for the pole step writing straight into the slot buffer
+(``b3d_pole_level``), then the caller's hook (the derivative moments).  Constants are built once per
+operator: the M-matrix table, the exact Q values with their sign, q L for every (L, Q) pair of the plan,
+and the R and q L tables aligned per row for the pole step.
+"""
+from fractions import Fraction
+
+import numpy as np
+import torch
+
+from . import _lib, mpf, structure as S
+from .mpf import MPF
+
+
+def _dev(a, device):
+    return torch.as_tensor(np.ascontiguousarray(a), dtype=torch.int64).to(device)
+
+
+class Recursion:
+    """Numbers of one Plan on the GPU.  M: dict key -> matrix of decimal strings (keys as plan.Mkeys),
+    an MPF table (nM, Smax, Smax) in plan.Mkeys order, or None for random O(1) matrices (timing runs)."""
+
+    def __init__(self, plan, M, L, device="cuda", generator=None):
+        if not _lib.lib().b3d_supported_limbs(L):
+            raise _lib.B3DError(f"no kernels compiled for L = {L}")
+        if plan.dmax >= 1 << 16:
+            raise _lib.B3DError(f"Cauchy differences up to {plan.dmax} exceed the one-limb kernel (< 65536)")
+        self.plan, self.L, self.device = plan, L, torch.device(device)
+        Sm, nM = plan.Smax, len(plan.Mkeys)
+        if M is None:
+            self.Mtab = mpf.random_mpf((nM, Sm, Sm), L, spread=1, device=self.device, generator=generator)
+        elif isinstance(M, MPF):
+            self.Mtab = M.to(self.device)
+        else:
+            strs = ["0"] * (nM * Sm * Sm)
+            for key, i in plan.Mkeys.items():
+                for a, row in enumerate(M.get(key) or []):
+                    for b, x in enumerate(row):
+                        strs[(i * Sm + a) * Sm + b] = x
+            self.Mtab = mpf.from_strings(strs, L, (nM, Sm, Sm), self.device)
+        self._constants()
+
+    def _constants(self):
+        plan, L, dev, Sm = self.plan, self.L, self.device, self.plan.Smax
+        qv = [Fraction(0)] * len(plan.Qkeys)
+        for (P, tj, sign), i in plan.Qkeys.items():
+            qv[i] = S.residue_prefactor(P, tj) * sign
+        self.Qtab = mpf.from_fractions(qv, L, (len(qv),), dev)
+        nlq = len(plan.LQpairs)
+        pairs = torch.as_tensor(plan.LQpairs, dtype=torch.int64, device=dev).reshape(nlq, 2)
+        s2 = torch.arange(Sm * Sm, device=dev)
+        aidx = (pairs[:, 0:1] * Sm * Sm + s2).reshape(-1)
+        bidx = pairs[:, 1:2].expand(nlq, Sm * Sm).reshape(-1)
+        QL = mpf.mul(self.Mtab.reshape(-1), self.Qtab, aidx=aidx, bidx=bidx, shape=(nlq, Sm, Sm))
+        self.Ralign = mpf.align_rows(self.Mtab)        # (L, nM, S, S), (nM, S)
+        self.QLalign = mpf.align_rows(QL)
+        self.levels = []
+        for lev in plan.levels:
+            if lev is None:
+                self.levels.append(None)
+                continue
+            d = {k: _dev(lev[k], dev) for k in ("gsrc", "gj", "rowd", "nrow", "cold", "ncol", "col",
+                                                   "t_slot", "t_hrow", "t_R", "t_qL")}
+            d.update(m=lev["m"], nb=lev["nb"], Mr=lev["Mr"], Kc=lev["Kc"], T=len(lev["t_slot"]))
+            self.levels.append(d)
+        live = [d for d in self.levels if d]
+        self.max_rows = max((d["nb"] * d["Mr"] for d in live), default=0)
+        self.max_tasks = max((d["T"] for d in live), default=0)
+
+    def footprint_bytes(self, B):
+        """device bytes run() allocates for B right-hand sides (slots, Cauchy rows, pole scratch)"""
+        per = (4 * self.L + 8) * self.plan.Smax ** 2 * B
+        return per * (self.plan.nphys + 1 + self.max_rows + self.max_tasks)
+
+    def run(self, h_inf, hook=None):
+        """h_inf: MPF (2, >= order, Jh, Smax^2, B).  Returns the residue slots MPF (nphys + 1, Smax^2, B);
+        hook(m, res) runs after each level (e.g. Derivs.accumulate)."""
+        plan, L, Sm = self.plan, self.L, self.plan.Smax
+        S2, B = Sm * Sm, h_inf.shape[-1]
+        N = S2 * B
+        hlevels = h_inf.shape[1]
+        if h_inf.L != L or h_inf.shape[2] < plan.Jh or hlevels < plan.order or h_inf.shape[3] != S2:
+            raise ValueError(f"h_inf shape {h_inf.shape} (L={h_inf.L}) does not match the plan")
+        h_inf = h_inf.contiguous()
+        Jh = h_inf.shape[2]
+        dev = self.device
+        res = mpf.zeros((plan.nphys + 1, S2, B), L, dev)
+        H = mpf.zeros((max(1, self.max_rows), N), L, dev)
+        Y = mpf.zeros((max(1, self.max_tasks), S2, B), L, dev)
+        stream = torch.cuda.current_stream(dev).cuda_stream
+        p = lambda t: t.data_ptr()
+        for lev in self.levels:
+            if lev is None:
+                continue
+            tabs = _lib.LevelTables(lev["m"], lev["nb"], lev["Mr"], lev["Kc"], N, hlevels, Jh,
+                                    p(lev["gsrc"]), p(lev["gj"]), p(lev["rowd"]), p(lev["nrow"]),
+                                    p(lev["cold"]), p(lev["ncol"]), p(lev["col"]))
+            _lib.call("b3d_cauchy_level", L, p(res.m), p(res.e), res.m.stride(0), p(h_inf.m), p(h_inf.e),
+                      h_inf.m.stride(0), _lib.ctypes_byref(tabs), p(H.m), p(H.e), H.m.stride(0), stream)
+            _lib.call("b3d_pole_level", L, p(H.m), p(H.e), H.m.stride(0),
+                      p(self.Ralign[0]), p(self.Ralign[1]), self.Ralign[0].stride(0),
+                      p(self.QLalign[0]), p(self.QLalign[1]), self.QLalign[0].stride(0),
+                      p(lev["t_hrow"]), p(lev["t_R"]), p(lev["t_qL"]), p(lev["t_slot"]), lev["T"], B, Sm,
+                      p(Y.m), p(Y.e), Y.m.stride(0), p(res.m), p(res.e), res.m.stride(0), stream)
+            if hook is not None:
+                hook(lev["m"], res)
+        return res
+
+    def slot(self, p, m, jidx, pidx):
+        """physical slot of residue (p, m, jidx, pidx) (meaningful after run() only without slot reuse)"""
+        return self.plan.phys_slot(p * self.plan.nslots + self.plan.offset(m, jidx) + pidx)

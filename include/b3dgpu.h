@@ -1,0 +1,105 @@
+/* C ABI of libb3dgpu.so: the B200 (sm_100a) kernels of blocks_3d's drop-in hot path.
+ *
+ * Numbers are multiprecision floats stored as limb planes: element i of an array with plane stride P has
+ * limbs m[k * P + i] (k = 0 .. L-1, 32-bit two's complement, limb 0 least significant) and exponent e[i];
+ * its value is m * 2^e.  Normalised values have |m| of exactly 32 L - 2 bits; zero is m = 0 with
+ * e = B3D_EZ.  All pointers are device pointers owned by the caller (PyTorch tensors on the host side);
+ * index arrays are int64.  `stream` is a cudaStream_t (NULL: the legacy default stream).  Every function
+ * returns 0 on success, B3D_E_LIMBS for a limb count without compiled kernels, B3D_E_ARG for invalid
+ * sizes, or a positive cudaError_t; b3d_last_error() describes the last failure of the calling thread.
+ * Nothing here allocates device memory.
+ */
+#ifndef B3DGPU_H
+#define B3DGPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define B3D_EZ (-(((int64_t)1) << 60))
+#define B3D_E_LIMBS (-1)
+#define B3D_E_ARG (-2)
+
+/* library version (major * 10000 + minor * 100 + patch) */
+int b3d_version(void);
+
+/* description of the last failure of the calling thread ("" if none) */
+const char* b3d_last_error(void);
+
+/* 1 if kernels are compiled for L limbs, else 0 */
+int b3d_supported_limbs(int L);
+
+/* Exponent alignment, the first half of sdpvibe's mpf.gemm / mpf._align_rows as called by the reference
+ * (recursion_gpu.py:53-70, smallgemm.py:154-175): for each (batch b, row r) of the strided view
+ * X[b, r, k] = element (bidx ? bidx[b] : b) * sb + r * sr + k * sk (k < K), write the mantissas shifted to
+ * the row's largest exponent (truncated below it) to om at (b * R + r) * K + k, or (b * K + k) * R + r
+ * when kmajor != 0, and the row exponents to oe[b * R + r]. */
+int b3d_align(int L, const int32_t* m, const int64_t* e, int64_t plane, int64_t nbatch, int64_t R, int64_t K,
+              int64_t sb, int64_t sr, int64_t sk, const int64_t* bidx, int32_t* om, int64_t* oe, int64_t oplane,
+              int kmajor, void* stream);
+
+/* Batched multiprecision GEMM on aligned operands, the second half of mpf.gemm (reference
+ * recursion_gpu.py:53 gemm, :73 bgemm; smallgemm.py:18-56): C[b, i, j] = sum_k A[b, i, k] B[b, k, j] with
+ * A = (am (b, M, K) row-aligned, ae (b, M)) and B = (bm (b, K, N) column-aligned, be (b, N)); exact
+ * products and sums, one rounding; C contiguous (b, M, N). */
+int b3d_gemm_aligned(int L, const int32_t* am, const int64_t* ae, int64_t aplane, const int32_t* bm,
+                     const int64_t* be, int64_t bplane, int64_t nbatch, int64_t M, int64_t N, int64_t K,
+                     int32_t* cm, int64_t* ce, int64_t cplane, void* stream);
+
+/* Elementwise C[i] = A[aidx ? aidx[i] : i] * B[bidx ? bidx[i] : i] (mpf.mul: exact product, one rounding;
+ * reference recursion_gpu.py:435, derivatives.py:496, :572) */
+int b3d_mul(int L, const int32_t* am, const int64_t* ae, int64_t aplane, const int64_t* aidx,
+            const int32_t* bm, const int64_t* be, int64_t bplane, const int64_t* bidx, int64_t n,
+            int32_t* cm, int64_t* ce, int64_t cplane, void* stream);
+
+/* Elementwise C[i] = A[..] + B[..] (mpf.add: one rounding; reference recursion_gpu.py:457, derivatives.py:573) */
+int b3d_add(int L, const int32_t* am, const int64_t* ae, int64_t aplane, const int64_t* aidx,
+            const int32_t* bm, const int64_t* be, int64_t bplane, const int64_t* bidx, int64_t n,
+            int32_t* cm, int64_t* ce, int64_t cplane, void* stream);
+
+/* Per-level tables of the Cauchy step (reference recursion_gpu.py:242-245 level dict, :368-376 tables) */
+typedef struct b3d_level_tables {
+    int64_t m, nb, Mr, Kc, N;      /* level, groups, rows per group, columns per group, S^2 B */
+    int64_t hlevels, Jh;           /* h_inf layout (2, hlevels, Jh, N) */
+    const int64_t* gsrc;           /* (nb) */
+    const int64_t* gj;             /* (nb) */
+    const int64_t* rowd;           /* (nb, Mr) 2 D' */
+    const int64_t* nrow;           /* (nb) */
+    const int64_t* cold;           /* (nb, Kc) 2 D_i */
+    const int64_t* ncol;           /* (nb) */
+    const int64_t* col;            /* (nb, Kc) physical slots */
+} b3d_level_tables;
+
+/* Cauchy step of one recursion level fused with the h_inf term (replaces cauchy.cauchy, cauchy.py:73-87,
+ * and recursion_gpu.py:451-460 + mpf.add): H[g, r, n] = hinf[gsrc[g], m, gj[g], n]
+ * + sum_i 2 / (rowd[g, r] - cold[g, i]) res[col[g, i], n].  res: (nslots, N), hinf: (2, hlevels, Jh, N),
+ * H: (nb, Mr, N).  |rowd - cold| must be < 65536. */
+int b3d_cauchy_level(int L, const int32_t* rm, const int64_t* re, int64_t rplane, const int32_t* hm,
+                     const int64_t* he, int64_t hplane, const b3d_level_tables* lv, int32_t* om, int64_t* oe,
+                     int64_t oplane, void* stream);
+
+/* Pole step of one recursion level (replaces Recursion._pole with pole="cuda", recursion_gpu.py:483-492,
+ * and the slot scatter :471-472): for each task t, res[t_slot[t]] = QL[t_qL[t]] (H[t_hrow[t]] R[t_R[t]]^T)
+ * with H: (rows, S, S, B), Rtab / QLtab: (n, S, S) row-aligned with row exponents (n, S) (b3d_align),
+ * scratch Y: (T, S, S, B), res: (nslots, S, S, B). */
+int b3d_pole_level(int L, const int32_t* hm, const int64_t* he, int64_t hplane, const int32_t* Rm,
+                   const int64_t* Re, int64_t Rplane, const int32_t* Qm, const int64_t* Qe, int64_t Qplane,
+                   const int64_t* t_hrow, const int64_t* t_R, const int64_t* t_qL, const int64_t* t_slot,
+                   int64_t T, int64_t B, int S, int32_t* ym, int64_t* ye, int64_t yplane, int32_t* rm,
+                   int64_t* re, int64_t rplane, void* stream);
+
+/* Derivative moments of one recursion level (replaces Derivs.accumulate + momacc, derivatives.py:48-96,
+ * :486-510): for each entry q and column c, y = res[q_slot[q], c] * rcpow[q_n[q]] and
+ * mom[q_row[q], k, c] += q_n[q]^k y for k < R1.  res: (nslots, N), rcpow: (order + 1), mom: (rows, R1, N). */
+int b3d_moments_level(int L, const int32_t* rm, const int64_t* re, int64_t rplane, const int32_t* pm,
+                      const int64_t* pe, int64_t pplane, const int64_t* q_slot, const int64_t* q_row,
+                      const int64_t* q_n, int64_t Q, int64_t N, int R1, int32_t* mm, int64_t* me, int64_t mplane,
+                      void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* B3DGPU_H */

@@ -1,0 +1,47 @@
+"""Oracle radial recursion: blocks_3d's fill_residues / set_residue, level by level, one (spin, pole,
+parity) at a time, in mpmath.  Restates the reference's exact CPU port recursion_ref.py:11-44.
+Test infrastructure only.
+
+Inputs: h_inf[(src, m, jh, a, b)] and M[(pole, side, tjNN, ppq, tj)] -> matrix (list of rows) of mpmath
+numbers; missing entries are zero.  Output: res[(p, m, jidx, pole index, a, b)].
+"""
+import mpmath as mp
+
+from . import blocks as B
+
+
+def fill_residues(h_inf, M, tj12, tj43, tj_max, order, pseudo_parities):
+    zero = mp.mpf(0)
+    res = {}
+    for m in range(order):
+        for jidx, tj in enumerate(B.spins(m, order, tj12, tj_max)):
+            for pidx, P in enumerate(B.pole_list(tj, tj12, tj43, order - m - B.excess(tj, tj_max))):
+                tjc = B.child(P, tj)
+                d_row = B.twice_pos(P, tj) + 2 * B.shift(P)
+                exc = B.excess(tjc, tj_max)
+                terms = []
+                for i in B.pole_list(tjc, tj12, tj43, m):
+                    diff = d_row - B.twice_pos(i, tjc)
+                    coef = mp.mpf(2) / diff if diff else zero
+                    pos = B.pole_list(tjc, tj12, tj43, order - m + B.shift(i) - exc).index(i)
+                    terms.append((m - B.shift(i), pos, coef))
+                q = B.q_value(P, tj)
+                qv = mp.mpf(q.numerator) / q.denominator
+                if (tjc - tj) % 4:
+                    qv = -qv
+                for p in range(2):
+                    src = (p + (1 if P[0] == 3 else 0)) % 2
+                    left = M.get((P, 0, tj12, pseudo_parities[src][0], tj))
+                    right = M.get((P, 1, tj43, pseudo_parities[src][1], tj))
+                    if not left or not left[0] or not right or not right[0]:
+                        continue
+                    nl, nr = len(left[0]), len(right[0])
+                    jc = tjc // 2
+                    h = [[h_inf.get((src, m, jc, a, b), zero)
+                          + mp.fsum(res.get((src, mm, jc, pos, a, b), zero) * c for mm, pos, c in terms)
+                          for b in range(nr)] for a in range(nl)]
+                    for a0 in range(len(left)):
+                        for b0 in range(len(right)):
+                            res[(p, m, jidx, pidx, a0, b0)] = qv * mp.fsum(
+                                left[a0][a] * h[a][b] * right[b0][b] for a in range(nl) for b in range(nr))
+    return res
