@@ -146,7 +146,13 @@ def from_fractions(fracs, L, shape=None, device=None):
 
 
 def _mp_parts(x):
-    sign, man, exp, _ = mp.mpf(x)._mpf_
+    """exact (mantissa, exponent) of an mpmath number or a Python int (never rounded to mpmath's
+    working precision)"""
+    if isinstance(x, int):
+        return x, 0
+    if not isinstance(x, mp.mpf):
+        raise TypeError(f"expected an mpmath mpf or an int, got {type(x).__name__}")
+    sign, man, exp, _ = x._mpf_
     if man == 0 and exp != 0:
         raise ValueError(f"not a finite number: {x}")
     return (-man if sign else man), exp
