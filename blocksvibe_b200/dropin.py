@@ -1,0 +1,158 @@
+"""The drop-in boundary of the hot path: the contract of the reference's ``cli._gpu``
+(``blocksvibe/cli.py:375-440``).  A *group* is a set of blocks_3d tasks sharing (j_external, j12, j43,
+Delta_12, Delta_43, order, Lambda, j_max, precision, kept_pole_order); its setup data are the M matrices
+and, per task, h_infinity for each lambda order (what the reference reads from b3d_setup's B3DSETUP file,
+``setup.py:128-180``).  ``run_group`` returns, per task, the write_output results as host limb arrays, the
+format ``cli._write_one`` hands to the JSON writer:
+
+    {(q4, sign): (two_js, pp, {(coord, d12): (m (L, Jo, 2, S^2, outputs, Dmax) int32,
+                                              e (Jo, 2, S^2, outputs, Dmax) int64)}, outputs, Smax, 32 L - 2)}
+
+Two schedules over the same kernels:
+  plain    one right-hand side batch per lambda order (all structures of a (pp, sign) subgroup), R = Lambda - n
+           per order: the reference's loop (cli.py:415-426);
+  batched  every (structure, lambda order) of a subgroup in ONE recursion pass (B = structures x orders),
+           moments accumulated once with R = Lambda - parity, numerators finished per lambda order from the
+           first R_n + 1 moments (the same sums: the moment of order k only depends on k).
+"""
+from dataclasses import dataclass, field
+
+import numpy as np
+import torch
+
+from . import mpf
+from .derivatives import Derivs
+from .mpf import MPF
+from .output import Output, apply_per_order
+from .plan import Plan
+from .recursion import Recursion
+
+
+@dataclass
+class Group:
+    two_js: tuple                 # external spins (doubled)
+    two_j12: int
+    two_j43: int
+    order: int
+    Lambda: int
+    two_j_max: int
+    precision: int
+    kept_pole_order: int
+    delta_12: str = "0"
+    delta_43: str = "0"
+
+
+@dataclass
+class Task:
+    """one blocks_3d invocation of the group: four-point structure q4 (doubled), sign, pseudo-parity types,
+    internal spins, coordinates, Delta_1+2, and h_inf per lambda order n: MPF (2, order + 1, Jh, Smax^2)"""
+    q4: tuple
+    sign: int
+    pp: tuple
+    two_js_internal: list
+    coordinates: tuple
+    delta_1_plus_2: str
+    h_inf: dict = field(default_factory=dict)
+
+    @property
+    def parity(self):
+        return (1 - self.sign) // 2
+
+    def lambda_orders(self, Lam):
+        radial = all(c.endswith("_radial") for c in self.coordinates)
+        return [self.parity] if radial else list(range(self.parity, Lam + 1, 2))
+
+
+def limbs(precision):
+    return mpf.limbs_for_precision(precision)
+
+
+class Operator:
+    """Plan + recursion constants + derivative constants + write_output maps of one (pp, sign) subgroup,
+    built once and reused for every batch (the reference rebuilds them per subgroup: cli.py:401-406)."""
+
+    def __init__(self, group, pp, parity, M, two_js, coords, d12s, device="cuda"):
+        self.group, self.pp, self.parity = group, pp, parity
+        self.L = limbs(group.precision)
+        self.plan = Plan(group.two_j12, group.two_j43, group.two_j_max, group.order, pp, reuse=True)
+        self.rec = Recursion(self.plan, M, self.L, device=device)
+        self.der = Derivs(self.plan, group.Lambda - parity, self.L, two_js=two_js,
+                          kept_pole_order=group.kept_pole_order, device=device)
+        self.outs = {(c, d): Output(c, group.Lambda, parity, d, self.L, device) for c in coords for d in d12s}
+        self.device = torch.device(device)
+
+    def footprint_bytes(self, B):
+        return self.rec.footprint_bytes(B) + self.der.footprint_bytes(B) + \
+            (4 * self.L + 8) * 2 * (self.group.order + 1) * self.plan.Jh * self.plan.Smax ** 2 * B
+
+    def hinf_batch(self, tasks, ns):
+        """h_inf MPF (2, order + 1, Jh, S^2, len(tasks) * len(ns)), rhs index = task * len(ns) + order index"""
+        cols = [t.h_inf[n] for t in tasks for n in ns]
+        m = torch.stack([c.m for c in cols], -1).to(self.device, non_blocking=True)
+        e = torch.stack([c.e for c in cols], -1).to(self.device, non_blocking=True)
+        return MPF(m, e)
+
+    def run_plain(self, tasks, ns):
+        """reference schedule: per lambda order one recursion over the structures; returns per-order numerators"""
+        G = self.group
+        nums = []
+        for n in ns:
+            d = self.der.for_order(G.Lambda - n)
+            h = self.hinf_batch(tasks, [n])
+            d.start(len(tasks))
+            self.rec.run(h, hook=d.accumulate)
+            nums.append(d.finish(h))
+        return nums
+
+    def run_batched(self, tasks, ns):
+        """one recursion pass over every (structure, lambda order); numerators per order from the shared moments"""
+        G = self.group
+        nq, no = len(tasks), len(ns)
+        h = self.hinf_batch(tasks, ns)                                        # rhs = q * no + idx
+        d = self.der
+        d.start(nq * no)
+        self.rec.run(h, hook=d.accumulate)
+        S2 = self.plan.Smax ** 2
+        mom = d.mom.reshape(d.mom.shape[0], d.R + 1, S2, nq, no)
+        nums = []
+        for idx, n in enumerate(ns):
+            dn = d.for_order(G.Lambda - n)
+            R1 = dn.R + 1
+            dn.B, dn.N = nq, S2 * nq
+            dn.mom = MPF(mom.m[:, :, :R1, :, :, idx], mom.e[:, :R1, :, :, idx]).contiguous().reshape(-1, R1, S2 * nq)
+            hn = MPF(h.m.reshape(*h.m.shape[:-1], nq, no)[..., idx], h.e.reshape(*h.e.shape[:-1], nq, no)[..., idx]).contiguous()
+            nums.append(dn.finish(hn))
+        return nums
+
+    def apply_outputs(self, nums, d12):
+        return {c: apply_per_order(o, nums) for (c, dd), o in self.outs.items() if dd == d12}
+
+
+def run_group(group, tasks, M, device="cuda", schedule="batched", max_rhs=None):
+    """All tasks of one group on the GPU.  M: matrices for the plan's keys (dict of decimal strings or an MPF
+    table in plan.Mkeys order; per pseudo-parity subgroup: {pp: M}).  Returns the per-task host results
+    described in the module docstring."""
+    sub = {}
+    for t in tasks:
+        sub.setdefault((tuple(t.pp), t.sign), []).append(t)
+    results = {}
+    for (pp, sign), ts in sub.items():
+        parity = (1 - sign) // 2
+        ns = sorted(set().union(*[t.lambda_orders(group.Lambda) for t in ts]))
+        tjs = sorted(set().union(*[t.two_js_internal for t in ts]))
+        coords = [c for c in ("xt", "xt_radial") if any(c in t.coordinates for t in ts)]
+        d12s = sorted({t.delta_1_plus_2 for t in ts})
+        op = Operator(group, pp, parity, M[pp] if isinstance(M, dict) and pp in M else M, tjs, coords, d12s, device)
+        bmax = max_rhs or len(ts)
+        for c0 in range(0, len(ts), bmax):
+            ch = ts[c0:c0 + bmax]
+            nums = op.run_batched(ch, ns) if schedule == "batched" else op.run_plain(ch, ns)
+            vals = {}
+            for d12 in d12s:
+                for c, r in op.apply_outputs(nums, d12).items():          # (Jo, 2, S2, nq, outputs, Dmax)
+                    vals[(c, d12)] = (r.m.cpu().numpy(), r.e.cpu().numpy())
+            for q, t in enumerate(ch):
+                results[(tuple(t.q4), t.sign)] = (
+                    tjs, pp, {k: (m[:, :, :, :, q], e[:, :, :, q]) for k, (m, e) in vals.items()},
+                    {k: list(o.outputs) for k, o in op.outs.items()}, op.plan.Smax, 32 * op.L - 2)
+    return results

@@ -1,0 +1,107 @@
+"""The drop-in group runner end to end (recursion -> numerators per lambda order -> xt / xt_radial) against
+the oracle chain (fill_residues -> numerators -> write_output transforms), and the schedules against each
+other: the batched pass (all structures and lambda orders as one batch) gives the plain per-order results
+bit for bit, and a task's result is the same alone and in a mix with other tasks."""
+import random
+
+import mpmath as mp
+import numpy as np
+import pytest
+import torch
+
+from helpers import agreement_bits, oracle_numerators
+from blocksvibe_b200 import dropin as DI, mpf, plan as PL, structure as S
+from oracle import output as OO
+
+pytestmark = pytest.mark.gpu
+
+
+def make_group(tj12=2, tj43=2, tjmax=4, order=8, Lam=4, precision=256, kept=5, seed=7, nq=2,
+               coords=("xt", "xt_radial"), sign=1, pp=((0, 0), (1, 1)), d12="2.3"):
+    G = DI.Group((2, 2, 2, 2), tj12, tj43, order, Lam, tjmax, precision, kept)
+    L = DI.limbs(precision)
+    plan = PL.Plan(tj12, tj43, tjmax, order, pp)
+    rng = random.Random(seed)
+    digits = 32 * L // 3
+    with mp.workprec(32 * L + 64):
+        rstr = lambda: mp.nstr(mp.mpf(rng.uniform(-2, 2)) + mp.mpf(rng.random()) * mp.mpf(2) ** -150, digits)
+        M = {key: [[rstr() for _ in range(len(S.so3_structures(key[3], key[2], S.child_spin(key[0], key[4]))))]
+                   for _ in range(len(S.so3_structures((key[3] + S.pole_parity(key[0])) % 2, key[2], key[4])))]
+             for key in plan.Mkeys}
+        Sm = plan.Smax
+        tasks, hstr = [], {}
+        for q in range(nq):
+            t = DI.Task((q, 2, 2 - q, 0), sign, pp, list(range(0, tjmax + 1, 2)), coords, d12)
+            for n in t.lambda_orders(Lam):
+                strs = ["0"] * (2 * (order + 1) * plan.Jh * Sm * Sm)
+                ent = []
+                for sp in range(2):
+                    for m in range(order + 1):
+                        for j in range(plan.Jh):
+                            tj = tj12 % 2 + 2 * j
+                            for a in range(len(S.so3_structures(pp[sp][0], tj12, tj))):
+                                for b in range(len(S.so3_structures(pp[sp][1], tj43, tj))):
+                                    v = rstr()
+                                    strs[(((sp * (order + 1) + m) * plan.Jh + j) * Sm + a) * Sm + b] = v
+                                    ent.append([0, sp, m, j, a, b, v])
+                t.h_inf[n] = mpf.from_strings(strs, L, (2, order + 1, plan.Jh, Sm * Sm))
+                hstr[(q, n)] = ent
+            tasks.append(t)
+    return G, tasks, M, hstr, plan
+
+
+def test_dropin_matches_oracle_chain(cuda):
+    G, tasks, M, hstr, plan = make_group()
+    L = DI.limbs(G.precision)
+    res = DI.run_group(G, tasks, M, device=cuda, schedule="plain")
+    Sm = plan.Smax
+    t0 = tasks[0]
+    tjs, pp, vals, outputs, Smax, NB = res[(tuple(t0.q4), t0.sign)]
+    assert NB == 32 * L - 2 and Smax == Sm
+    ns = t0.lambda_orders(G.Lambda)
+    nums = {n: oracle_numerators(M, hstr[(0, n)], G.two_j12, G.two_j43, G.two_j_max, G.order, t0.pp, L, 0,
+                                 G.Lambda - n, tjs, G.kept_pole_order) for n in ns}
+    m, e = vals[("xt", t0.delta_1_plus_2)]
+    got_xt = mpf.to_mp(mpf.MPF(torch.from_numpy(m), torch.from_numpy(e)))      # (Jo, 2, S2, outputs, Dmax)
+    m, e = vals[("xt_radial", t0.delta_1_plus_2)]
+    got_rad = mpf.to_mp(mpf.MPF(torch.from_numpy(m), torch.from_numpy(e)))
+    worst = float("inf")
+    with mp.workprec(32 * L + 128):
+        for (tj, p, a, b), _ in nums[ns[0]].items():
+            jo = tjs.index(tj)
+            Dmax = got_xt.shape[-1]
+            for dcoef in range(Dmax):
+                # num[idx][e] for coefficient dcoef
+                table = []
+                for n in ns:
+                    polys = nums[n][(tj, p, a, b)]
+                    table.append([polys[ee][dcoef] if ee <= G.Lambda - n and dcoef < len(polys[ee]) else mp.mpf(0)
+                                  for ee in range(G.Lambda - t0.parity + 1)])
+                ref_xt = [x for row in OO.xt(table, G.Lambda, t0.parity, t0.delta_1_plus_2) for x in row]
+                ref_rad = OO.xt_radial(table[0], G.Lambda, t0.parity, t0.delta_1_plus_2)
+                g_xt = [got_xt[jo, p, a * Sm + b, o, dcoef] for o in range(len(ref_xt))]
+                g_rad = [got_rad[jo, p, a * Sm + b, o, dcoef] for o in range(len(ref_rad))]
+                for g, r in ((g_xt, ref_xt), (g_rad, ref_rad)):
+                    if max(abs(x) for x in r) == 0:
+                        continue
+                    worst = min(worst, agreement_bits(g, r))
+    assert worst > 32 * L - 40, worst
+
+
+def test_batched_schedule_is_bitwise_plain(cuda):
+    G, tasks, M, _, _ = make_group(nq=3, seed=9, coords=("xt",))
+    a = DI.run_group(G, tasks, M, device=cuda, schedule="plain")
+    b = DI.run_group(G, tasks, M, device=cuda, schedule="batched")
+    assert a.keys() == b.keys()
+    for k in a:
+        for c in a[k][2]:
+            assert np.array_equal(a[k][2][c][0], b[k][2][c][0]) and np.array_equal(a[k][2][c][1], b[k][2][c][1])
+
+
+def test_result_same_alone_and_in_mix(cuda):
+    G, tasks, M, _, _ = make_group(nq=3, seed=11, coords=("xt",), sign=-1)
+    mix = DI.run_group(G, tasks, M, device=cuda, schedule="batched")
+    alone = DI.run_group(G, tasks[1:2], M, device=cuda, schedule="batched")
+    k = (tuple(tasks[1].q4), tasks[1].sign)
+    for c in alone[k][2]:
+        assert np.array_equal(alone[k][2][c][0], mix[k][2][c][0]) and np.array_equal(alone[k][2][c][1], mix[k][2][c][1])
