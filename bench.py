@@ -1,0 +1,358 @@
+#!/usr/bin/env python
+"""Benchmark of the blocks_3d drop-in hot path on B200: blocks_3d tasks per second.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload cfg2] [--schedule batched|plain]
+    python bench.py --impl reference ...        the reference's CPU path (the oracle port) on the host cores
+
+A step is one blocks_3d task of the workload (default cfg2: external spins (2,2,2,2), 2 j12 = 2 j43 = 8,
+internal spins 0-22, Lambda 11, order 40, kept pole order 20, 1024 bits, xt; its six lambda orders are the
+task's right-hand sides): radial recursion with derivative moments, numerators with pole shifting, the xt
+map.  Inputs are synthetic (random M matrices and h_infinity: the cost does not depend on the values).
+The operator's constants (plan, M tables, derivative and write_output maps) are built once before timing,
+as they are once per group of tasks.  `value` times the step with h_inf already on the device; `e2e` times
+the same step through the drop-in runner's host interface: h_inf copied from pinned host memory and the
+write_output limbs copied back to the host inside the timed region.
+
+With N > 1 (torchrun), every rank runs the same workload on its own GPU (independent replicas: the path has no
+exchange step); the timing is the max over ranks and `value` counts the tasks of all ranks.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=("ours", "reference"))
+    ap.add_argument("--workload", default="cfg2")
+    ap.add_argument("--schedule", default="batched", choices=("batched", "plain"))
+    ap.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of the CPU-baseline sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------- distributed plumbing
+def dist_setup():
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x, world, device):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ---------------------------------------------------------------- clocks during the timed region
+class Clocks:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self):
+        self.path = tempfile.mktemp(suffix=".csv")
+        self.proc = None
+
+    def start(self):
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                                          "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self, gpu_index=0):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        self.proc.wait()
+        self.f.close()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9 or f[0] != str(gpu_index):
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        os.unlink(self.path)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------- kernel probe (launch count, per-kernel events)
+KERNELS_PER_CALL = {"b3d_pole_level": 2}
+
+
+class Probe:
+    """wraps the C ABI dispatcher: counts kernel launches and records CUDA events around the calls of one
+    entry point on the launching (current) stream"""
+
+    def __init__(self):
+        from blocksvibe_b200 import _lib
+        self.lib = _lib
+        self.orig = _lib.call
+        self.launches = 0
+        self.watch = None
+        self.events = []
+        self.by_name = None
+        _lib.call = self._call
+
+    def _call(self, name, *args):
+        import torch
+        self.launches += KERNELS_PER_CALL.get(name, 1)
+        timed = name == self.watch or self.by_name is not None
+        if timed:
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record()
+        rc = self.orig(name, *args)
+        if timed:
+            e.record()
+            if name == self.watch:
+                self.events.append((s, e))
+            if self.by_name is not None:
+                self.by_name.setdefault(name, []).append((s, e))
+        return rc
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d.get("hbm_gbs", 6650.0), "measured"
+    return 6650.0, "fallback"
+
+
+def profile_traffic(kernel, workload):
+    """dram bytes per launch of `kernel` from the committed ncu summary of this workload, if any"""
+    path = os.path.join(ROOT, "profiles", f"{kernel}_{workload}.md")
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        if line.startswith("traffic_bytes_per_launch:"):
+            return float(line.split(":")[1])
+    return None
+
+
+# ---------------------------------------------------------------- CPU baseline (oracle port on the host cores)
+def cpu_baseline(c, budget, cores):
+    from oracle import sample as OS
+    from blocksvibe_b200 import mpf
+    L = mpf.limbs_for_precision(c["precision"])
+    parity = (1 - c["sign"]) // 2
+    nrhs = len(range(parity, c["Lam"] + 1, 2)) if "xt" in c["coords"] else 1
+    per_rhs = OS.recursion_macs_per_rhs(c["tj12"], c["tj43"], c["tjmax"], c["order"], c["pp"])
+    macs, secs = OS.parallel_sample(c["tj12"], c["tj43"], c["tjmax"], c["order"], c["pp"], 32 * L + 64, budget, cores)
+    rate = macs / secs                                     # MP MACs per second over all workers
+    tasks_per_s = rate / (per_rhs * nrhs)
+    return {"value": tasks_per_s, "unit": "tasks/s", "cores": cores, "kind": "port",
+            "sample": (f"oracle fill_residues (mpmath, {32 * L + 64}-bit) on {cores} spawned processes for "
+                       f"{budget:.0f} s each, {macs:.3g} MP MACs done; tasks/s = MAC rate / ({per_rhs:.3g} recursion "
+                       f"MACs per right-hand side x {nrhs} lambda orders): recursion only, an upper bound on CPU tasks/s")}
+
+
+def run_reference(args):
+    """--impl reference: the reference's CPU path (the oracle port of recursion_ref) on the host cores"""
+    from blocksvibe_b200.workloads import CONFIGS
+    world, rank, _ = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0
+    if rank != 0:
+        return
+    c = CONFIGS[args.workload]
+    cores = os.cpu_count() or 1
+    budget = max(2.0, min(args.cpu_budget, 150.0 / max(1, args.steps + args.warmup)))
+    vals = []
+    for i in range(args.warmup + args.steps):
+        r = cpu_baseline(c, budget, cores)
+        if i >= args.warmup:
+            vals.append(r["value"])
+    v = statistics.mean(vals)
+    r["value"] = v
+    line = {"impl": "reference", "metric": "blocks_3d tasks/s", "value": v, "unit": "tasks/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / v, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "mpf (mpmath)", "data": "synthetic",
+            "config": {"workload": args.workload, **{k: c[k] for k in ("tj12", "tj43", "tjmax", "Lam", "order", "kept", "precision")}},
+            "cpu_baseline": r, "e2e": {"value": v, "unit": "tasks/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------- our arm
+def run_ours(args):
+    import torch
+    from blocksvibe_b200 import dropin as DI, mpf, roofline as RL
+    from blocksvibe_b200.mpf import MPF
+    from blocksvibe_b200.workloads import CONFIGS, make_tasks
+
+    world, rank, local = dist_setup()
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    c = CONFIGS[args.workload]
+    G, tasks = make_tasks(c, nq=1, seed=rank)
+    t = tasks[0]
+    parity = t.parity
+    ns = t.lambda_orders(G.Lambda)
+    t_setup = time.perf_counter()
+    op = DI.Operator(G, t.pp, parity, None, t.two_js_internal, list(t.coordinates), [t.delta_1_plus_2], dev)
+    torch.cuda.synchronize()
+    t_setup = time.perf_counter() - t_setup
+    dtask = DI.Task(t.q4, t.sign, t.pp, t.two_js_internal, t.coordinates, t.delta_1_plus_2,
+                    {n: MPF(h.m.to(dev), h.e.to(dev)) for n, h in t.h_inf.items()})
+    run = op.run_batched if args.schedule == "batched" else op.run_plain
+
+    def step_device():
+        nums = run([dtask], ns)
+        return op.apply_outputs(nums, t.delta_1_plus_2)
+
+    h2d = sum(h.m.numel() * 4 + h.e.numel() * 8 for h in t.h_inf.values())
+    d2h = [0]
+
+    def step_e2e():
+        nums = run([t], ns)
+        outs = op.apply_outputs(nums, t.delta_1_plus_2)
+        host = {k: (r.m.cpu(), r.e.cpu()) for k, r in outs.items()}
+        d2h[0] = sum(m.numel() * 4 + e.numel() * 8 for m, e in host.values())
+        return host
+
+    probe = Probe()
+    # per-kernel split (one untimed step) to pick the dominant kernel
+    probe.by_name = {}
+    step_device()
+    torch.cuda.synchronize()
+    split = {k: sum(s.elapsed_time(e) for s, e in v) for k, v in probe.by_name.items()}
+    probe.by_name = None
+    dominant = max(split, key=split.get)
+
+    for _ in range(args.warmup):
+        step_device()
+    clocks = Clocks()
+    torch.cuda.synchronize()
+    barrier(world)
+    torch.cuda.synchronize()
+    if rank == 0:
+        clocks.start()
+    probe.watch, probe.events = dominant, []
+    n0 = probe.launches
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record()
+    for _ in range(args.steps):
+        step_device()
+    end.record()
+    torch.cuda.synchronize()
+    barrier(world)
+    ms = start.elapsed_time(end) / args.steps
+    launches = (probe.launches - n0) // args.steps
+    kernel_ms = [s.elapsed_time(e) for s, e in probe.events]
+    probe.watch = None
+    clk = clocks.stop(local) if rank == 0 else None
+    ms = max_over_ranks(ms, world, dev)
+
+    # end to end through the host interface, per-step latencies for p50 / p99
+    for _ in range(args.warmup):
+        step_e2e()
+    torch.cuda.synchronize()
+    barrier(world)
+    lat = []
+    e0 = time.perf_counter()
+    for _ in range(args.steps):
+        s = time.perf_counter()
+        step_e2e()
+        torch.cuda.synchronize()
+        lat.append(time.perf_counter() - s)
+    e2e_s = (time.perf_counter() - e0) / args.steps
+    barrier(world)
+    e2e_s = max_over_ranks(e2e_s, world, dev)
+
+    # roofline of the dominant kernel: algorithmic bytes per launch / mean launch time
+    L, N, S = op.L, op.plan.Smax ** 2 * (len(ns) if args.schedule == "batched" else 1), op.plan.Smax
+    levs = [lv for lv in op.plan.levels if lv]
+    if dominant == "b3d_cauchy_level":
+        per_step_bytes = sum(RL.cauchy_level_bytes(lv, N, L) for lv in levs) * (1 if args.schedule == "batched" else len(ns))
+    elif dominant == "b3d_pole_level":
+        per_step_bytes = sum(RL.pole_level_bytes(lv, N, S, L) for lv in levs) * (1 if args.schedule == "batched" else len(ns))
+    else:
+        per_step_bytes = None
+    hbm, peak_kind = peaks()
+    roof = None
+    if per_step_bytes and kernel_ms:
+        nl = len(kernel_ms) / args.steps
+        achieved = (per_step_bytes / nl) / (statistics.mean(kernel_ms) / 1e3) / 1e9
+        traffic = profile_traffic(dominant, args.workload)
+        roof = {"kernel": dominant, "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                "frac": achieved / hbm, "peak_source": peak_kind, "traffic": traffic,
+                "algorithmic_bytes_per_launch": per_step_bytes / nl, "mean_launch_ms": statistics.mean(kernel_ms)}
+    if rank != 0:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
+    cpu = None
+    if world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(c, args.cpu_budget, os.cpu_count() or 1)
+    lat.sort()
+    pct = lambda q: lat[min(len(lat) - 1, int(round(q * (len(lat) - 1))))] * 1e3
+    value = world / (ms / 1e3)
+    line = {"metric": "blocks_3d tasks/s", "value": value, "unit": "tasks/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "mpf int32 limbs", "data": "synthetic (random M and h_inf of the config's shape)",
+            "config": {"workload": args.workload, "schedule": args.schedule, "two_js": list(c["two_js"]),
+                       "two_j12": c["tj12"], "two_j43": c["tj43"], "two_j_max": c["tjmax"], "Lambda": c["Lam"],
+                       "order": c["order"], "kept_pole_order": c["kept"], "precision": c["precision"], "limbs": L,
+                       "coordinates": list(c["coords"]), "rhs_per_task": len(ns), "parallelism": f"replicas{world}",
+                       "l2": "inputs larger than L2 (residue slot buffer %.2f GB)" % (op.rec.footprint_bytes(len(ns)) / 1e9)},
+            "e2e": {"value": world / e2e_s, "unit": "tasks/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h[0]},
+            "latency_ms": {"p50": pct(0.5), "p99": pct(0.99), "source": "e2e steps"},
+            "gpu_launches": launches, "setup_s": t_setup,
+            "kernel_split_ms": {k: round(v, 3) for k, v in sorted(split.items(), key=lambda x: -x[1])},
+            "roofline": roof, "cpu_baseline": cpu, "clocks": clk}
+    print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -10,10 +10,19 @@ import mpmath as mp
 from . import blocks as B
 
 
-def fill_residues(h_inf, M, tj12, tj43, tj_max, order, pseudo_parities):
+def fill_residues(h_inf, M, tj12, tj43, tj_max, order, pseudo_parities, budget=None, stats=None):
+    """budget: stop after this many seconds (a bounded sample for CPU timing); stats: dict receiving the
+    multiprecision MACs done ("macs") and whether the run completed ("complete")"""
+    import time
+    t_end = None if budget is None else time.perf_counter() + budget
+    macs = 0
     zero = mp.mpf(0)
     res = {}
     for m in range(order):
+        if t_end is not None and time.perf_counter() > t_end:
+            if stats is not None:
+                stats.update(macs=macs, complete=False)
+            return res
         for jidx, tj in enumerate(B.spins(m, order, tj12, tj_max)):
             for pidx, P in enumerate(B.pole_list(tj, tj12, tj43, order - m - B.excess(tj, tj_max))):
                 tjc = B.child(P, tj)
@@ -44,4 +53,28 @@ def fill_residues(h_inf, M, tj12, tj43, tj_max, order, pseudo_parities):
                         for b0 in range(len(right)):
                             res[(p, m, jidx, pidx, a0, b0)] = qv * mp.fsum(
                                 left[a0][a] * h[a][b] * right[b0][b] for a in range(nl) for b in range(nr))
+                    macs += len(terms) * nl * nr + 2 * len(left) * len(right) * nl * nr
+                if t_end is not None and time.perf_counter() > t_end:
+                    break
+    if stats is not None:
+        stats.update(macs=macs, complete=t_end is None or time.perf_counter() <= t_end)
     return res
+
+
+def count_macs(tj12, tj43, tj_max, order, pseudo_parities, M_shapes):
+    """multiprecision MACs fill_residues does for one right-hand side (the count of its loops, no arithmetic);
+    M_shapes[key] = (rows, cols) of the matrices present"""
+    macs = 0
+    for m in range(order):
+        for jidx, tj in enumerate(B.spins(m, order, tj12, tj_max)):
+            for P in B.pole_list(tj, tj12, tj43, order - m - B.excess(tj, tj_max)):
+                nterms = len(B.pole_list(B.child(P, tj), tj12, tj43, m))
+                for p in range(2):
+                    src = (p + (1 if P[0] == 3 else 0)) % 2
+                    ls = M_shapes.get((P, 0, tj12, pseudo_parities[src][0], tj))
+                    rs = M_shapes.get((P, 1, tj43, pseudo_parities[src][1], tj))
+                    if not ls or not rs or not ls[1] or not rs[1]:
+                        continue
+                    nl, nr = ls[1], rs[1]
+                    macs += nterms * nl * nr + 2 * ls[0] * rs[0] * nl * nr
+    return macs
