@@ -4,15 +4,9 @@
 #include <string>
 
 #include "b3dgpu.h"
-#include "kernels.cuh"
+#include "abi_internal.h"
 
 namespace b3d {
-#define B3D_DECL(L) extern template struct Launch<L>;
-B3D_FOR_EACH_L(B3D_DECL)
-#undef B3D_DECL
-}  // namespace b3d
-
-namespace {
 
 thread_local std::string g_error;
 
@@ -26,19 +20,14 @@ int cuda_status(int code, const char* fn) {
     return fail(code, std::string(fn) + ": " + cudaGetErrorString((cudaError_t)code));
 }
 
-inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+}  // namespace b3d
 
-#define B3D_DISPATCH(L, CALL)                                                  \
-    switch (L) {                                                               \
-        case 6: { using LX = b3d::Launch<6>; return CALL; }                     \
-        case 10: { using LX = b3d::Launch<10>; return CALL; }                   \
-        case 18: { using LX = b3d::Launch<18>; return CALL; }                   \
-        case 26: { using LX = b3d::Launch<26>; return CALL; }                   \
-        case 30: { using LX = b3d::Launch<30>; return CALL; }                   \
-        case 34: { using LX = b3d::Launch<34>; return CALL; }                   \
-        case 42: { using LX = b3d::Launch<42>; return CALL; }                   \
-        default: return fail(B3D_E_LIMBS, "no kernels compiled for L = " + std::to_string(L)); \
-    }
+namespace {
+
+using b3d::cuda_status;
+using b3d::fail;
+
+inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
 
 bool nonneg(int64_t x) { return x >= 0; }
 
@@ -48,7 +37,7 @@ extern "C" {
 
 int b3d_version(void) { return 100; }
 
-const char* b3d_last_error(void) { return g_error.c_str(); }
+const char* b3d_last_error(void) { return b3d::g_error.c_str(); }
 
 int b3d_supported_limbs(int L) {
     switch (L) {

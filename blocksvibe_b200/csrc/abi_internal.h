@@ -1,0 +1,28 @@
+// Shared by the C ABI translation units: error reporting and the dispatch on the limb count.
+#pragma once
+#include <string>
+
+#include "kernels.cuh"
+
+namespace b3d {
+#define B3D_DECL(L) extern template struct Launch<L>;
+B3D_FOR_EACH_L(B3D_DECL)
+#undef B3D_DECL
+
+// record `what` as the calling thread's last error (b3d_last_error) and return `code`
+int fail(int code, const std::string& what);
+// 0 for cudaSuccess, else the error code with its message recorded
+int cuda_status(int code, const char* fn);
+}  // namespace b3d
+
+#define B3D_DISPATCH(L, CALL)                                                  \
+    switch (L) {                                                               \
+        case 6: { using LX = b3d::Launch<6>; return CALL; }                    \
+        case 10: { using LX = b3d::Launch<10>; return CALL; }                  \
+        case 18: { using LX = b3d::Launch<18>; return CALL; }                  \
+        case 26: { using LX = b3d::Launch<26>; return CALL; }                  \
+        case 30: { using LX = b3d::Launch<30>; return CALL; }                  \
+        case 34: { using LX = b3d::Launch<34>; return CALL; }                  \
+        case 42: { using LX = b3d::Launch<42>; return CALL; }                  \
+        default: return b3d::fail(B3D_E_LIMBS, "no kernels compiled for L = " + std::to_string(L)); \
+    }
