@@ -21,6 +21,7 @@ SIGNATURES = {
     "b3d_cauchy_level": [_I, _P, _P, _Q, _P, _P, _Q, _P, _P, _P, _Q, _P],
     "b3d_pole_level": [_I, _P, _P, _Q, _P, _P, _Q, _P, _P, _Q, _P, _P, _P, _P, _Q, _Q, _I, _P, _P, _Q, _P, _P, _Q, _P],
     "b3d_moments_level": [_I, _P, _P, _Q, _P, _P, _Q, _P, _P, _P, _Q, _Q, _I, _P, _P, _Q, _P],
+    "b3d_pole_level_noalloc": [_I, _P, _P, _Q, _P, _P, _Q, _P, _P, _Q, _P, _P, _P, _P, _Q, _Q, _I, _P, _P, _Q, _P],
 }
 
 

@@ -25,7 +25,7 @@ def _nvcc():
 
 
 def _sources():
-    return [os.path.join(CSRC, f) for f in sorted(os.listdir(CSRC)) if f.endswith((".cu", ".cuh"))] + \
+    return [os.path.join(CSRC, f) for f in sorted(os.listdir(CSRC)) if f.endswith((".cu", ".cuh", ".h"))] + \
            [os.path.join(ROOT, "include", "b3dgpu.h")]
 
 
@@ -51,7 +51,8 @@ def build(force=False, verbose=False):
     nvcc = _nvcc()
     jobs = [[nvcc, *ARCH, *FLAGS, f"-DB3D_L={L}", "-c", os.path.join(CSRC, "inst.cu"),
              "-o", os.path.join(BUILD, f"inst_L{L}.o")] for L in LIMBS]
-    jobs.append([nvcc, *ARCH, *FLAGS, "-c", os.path.join(CSRC, "abi.cu"), "-o", os.path.join(BUILD, "abi.o")])
+    for unit in ("abi", "noalloc"):
+        jobs.append([nvcc, *ARCH, *FLAGS, "-c", os.path.join(CSRC, f"{unit}.cu"), "-o", os.path.join(BUILD, f"{unit}.o")])
     with ThreadPoolExecutor(max_workers=min(len(jobs), os.cpu_count() or 4)) as ex:
         for log in ex.map(_run, jobs):
             if verbose and log:

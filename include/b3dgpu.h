@@ -12,6 +12,7 @@
 #ifndef B3DGPU_H
 #define B3DGPU_H
 
+#include <stddef.h>
 #include <stdint.h>
 
 #ifdef __cplusplus
@@ -97,6 +98,21 @@ int b3d_moments_level(int L, const int32_t* rm, const int64_t* re, int64_t rplan
                       const int64_t* pe, int64_t pplane, const int64_t* q_slot, const int64_t* q_row,
                       const int64_t* q_n, int64_t Q, int64_t N, int R1, int32_t* mm, int64_t* me, int64_t mplane,
                       void* stream);
+
+/* Size of the device scratch array of b3d_pole_level_noalloc (per GPU, held until the process exits). */
+#define B3D_NOALLOC_SCRATCH_BYTES ((size_t)16 << 20)
+
+/* b3d_pole_level without a caller-provided scratch buffer (no counterpart in the reference: an addition for
+ * callers that cannot allocate device memory while they run, e.g. when another allocator owns the device
+ * memory or a serving loop budgets it per request).  Same arguments and results as b3d_pole_level minus
+ * ym / ye / yplane; the intermediate lives in a fixed array of B3D_NOALLOC_SCRATCH_BYTES, so a call needs
+ * T * S^2 * B * (4 L + 8) <= B3D_NOALLOC_SCRATCH_BYTES - 256 bytes (else B3D_E_ARG: split the level's tasks).
+ * Allocates nothing.  The first call on each device looks the array's address up: make it before any stream
+ * capture.  All calls on a device share the array: calls whose kernels overlap on the GPU race. */
+int b3d_pole_level_noalloc(int L, const int32_t* hm, const int64_t* he, int64_t hplane, const int32_t* Rm,
+                           const int64_t* Re, int64_t Rplane, const int32_t* Qm, const int64_t* Qe, int64_t Qplane,
+                           const int64_t* t_hrow, const int64_t* t_R, const int64_t* t_qL, const int64_t* t_slot,
+                           int64_t T, int64_t B, int S, int32_t* rm, int64_t* re, int64_t rplane, void* stream);
 
 #ifdef __cplusplus
 }
