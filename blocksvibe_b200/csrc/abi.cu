@@ -109,4 +109,50 @@ int b3d_moments_level(int L, const int32_t* rm, const int64_t* re, int64_t rplan
                                            mplane, as_stream(stream)), "b3d_moments_level"));
 }
 
+namespace {
+b3d::RnsTables tables_of(const b3d_rns_tables* t) {
+    return b3d::RnsTables{t->p, t->mu, t->w, t->conv, t->inv, t->mj, t->mfull, t->rp, t->np, t->ml};
+}
+}  // namespace
+
+int b3d_rns_layout(int L, int* np, int* ml) {
+    if (!b3d_supported_limbs(L)) return fail(B3D_E_LIMBS, "no kernels compiled for L = " + std::to_string(L));
+    *np = b3d::rns_primes(L);
+    *ml = b3d::rns_mlimbs(L);
+    return 0;
+}
+
+int b3d_rns_split(int L, const int32_t* m, int64_t plane, int64_t nb, int64_t R, int64_t K, int64_t sb, int64_t sr,
+                  int64_t sk, int64_t Rp, int64_t Kp, int TR, const b3d_rns_tables* tb, uint8_t* out,
+                  int64_t mat_bytes, void* stream) {
+    if (!tb || nb < 0 || R < 0 || K < 0 || Rp < R || Kp < K || Kp % 32 || TR % 16 || TR <= 0 || (4 * Rp) % TR ||
+        mat_bytes < 4 * Rp * Kp || tb->np != b3d::rns_primes(L))
+        return fail(B3D_E_ARG, "b3d_rns_split: invalid sizes or tables");
+    b3d::RnsTables t = tables_of(tb);
+    B3D_DISPATCH_RNS(L, cuda_status(RX::split(m, plane, nb, R, K, sb, sr, sk, Rp, Kp, TR, t, out, mat_bytes,
+                                              as_stream(stream)), "b3d_rns_split"));
+}
+
+int b3d_rns_mma(const b3d_rns_mma_args* a, const b3d_rns_tables* tb, void* stream) {
+    if (!a || !tb || a->Kp <= 0 || a->Kp > 256 || a->Kp % 32 || a->TN < 16 || a->TN > 256 || a->TN % 16 ||
+        a->nb <= 0 || a->nb > 65535 || tb->np <= 0 || tb->np > 65535 || a->NI < 0 || a->NL < 0 ||
+        a->tiles_l * (a->TN / 4) < a->NL || a->x_mat < ((4 * a->NI + 127) / 128) * 128 * (int64_t)a->Kp ||
+        a->y_mat < a->tiles_l * a->TN * (int64_t)a->Kp)
+        return fail(B3D_E_ARG, "b3d_rns_mma: invalid sizes");
+    if (a->NI == 0 || a->NL == 0) return 0;
+    b3d::RnsMma m{a->X, a->Y, a->x_mat, a->y_mat, a->nb, a->NI, a->NL, a->Kp, a->TN, a->tiles_l, a->out_b, a->out_i,
+                  a->out_l, a->out, a->err};
+    return cuda_status(b3d::rns_mma_launch(m, tables_of(tb), as_stream(stream)), "b3d_rns_mma");
+}
+
+int b3d_rns_crt(int L, const uint32_t* res, int64_t n, const int64_t* ea, const int64_t* eb, int64_t nbatch,
+                int64_t M, int64_t N, const b3d_rns_tables* tb, int32_t* cm, int64_t* ce, int64_t cplane,
+                void* stream) {
+    if (!tb || n != nbatch * M * N || n < 0 || tb->np != b3d::rns_primes(L) || tb->ml != b3d::rns_mlimbs(L))
+        return fail(B3D_E_ARG, "b3d_rns_crt: invalid sizes or tables");
+    b3d::RnsTables t = tables_of(tb);
+    B3D_DISPATCH_RNS(L, cuda_status(RX::crt(res, n, ea, eb, nbatch, M, N, t, cm, ce, cplane, as_stream(stream)),
+                                    "b3d_rns_crt"));
+}
+
 }  // extern "C"

@@ -3,9 +3,10 @@
 #include <string>
 
 #include "kernels.cuh"
+#include "rns.cuh"
 
 namespace b3d {
-#define B3D_DECL(L) extern template struct Launch<L>;
+#define B3D_DECL(L) extern template struct Launch<L>; extern template struct RnsLaunch<L>;
 B3D_FOR_EACH_L(B3D_DECL)
 #undef B3D_DECL
 
@@ -13,7 +14,21 @@ B3D_FOR_EACH_L(B3D_DECL)
 int fail(int code, const std::string& what);
 // 0 for cudaSuccess, else the error code with its message recorded
 int cuda_status(int code, const char* fn);
+// tensor-core residue product (rns_mma.cu)
+int rns_mma_launch(const RnsMma& a, const RnsTables& tb, cudaStream_t st);
 }  // namespace b3d
+
+#define B3D_DISPATCH_RNS(L, CALL)                                              \
+    switch (L) {                                                               \
+        case 6: { using RX = b3d::RnsLaunch<6>; return CALL; }                 \
+        case 10: { using RX = b3d::RnsLaunch<10>; return CALL; }               \
+        case 18: { using RX = b3d::RnsLaunch<18>; return CALL; }               \
+        case 26: { using RX = b3d::RnsLaunch<26>; return CALL; }               \
+        case 30: { using RX = b3d::RnsLaunch<30>; return CALL; }               \
+        case 34: { using RX = b3d::RnsLaunch<34>; return CALL; }               \
+        case 42: { using RX = b3d::RnsLaunch<42>; return CALL; }               \
+        default: return b3d::fail(B3D_E_LIMBS, "no kernels compiled for L = " + std::to_string(L)); \
+    }
 
 #define B3D_DISPATCH(L, CALL)                                                  \
     switch (L) {                                                               \

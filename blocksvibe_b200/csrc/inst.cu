@@ -1,6 +1,7 @@
 // One translation unit per limb count (compiled with -DB3D_L=<L>): instantiates the kernel launchers.
 #define B3D_DEFINE_LAUNCH
 #include "kernels.cuh"
+#include "rns.cuh"
 
 #ifndef B3D_L
 #error "compile with -DB3D_L=<limbs>"
@@ -8,4 +9,5 @@
 
 namespace b3d {
 template struct Launch<B3D_L>;
+template struct RnsLaunch<B3D_L>;
 }

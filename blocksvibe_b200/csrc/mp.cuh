@@ -17,14 +17,16 @@ typedef uint32_t u32;
 typedef uint64_t u64;
 typedef int64_t i64;
 
-constexpr i64 EZ = -(i64(1) << 60);       // exponent of zero
-constexpr int nb_bits(int L) { return 32 * L - 2; }
-
 #ifdef __CUDACC__
 #define B3D_HD __host__ __device__ __forceinline__
+#define B3D_CX __host__ __device__ constexpr
 #else
 #define B3D_HD inline
+#define B3D_CX constexpr
 #endif
+
+constexpr i64 EZ = -(i64(1) << 60);       // exponent of zero
+B3D_CX int nb_bits(int L) { return 32 * L - 2; }
 
 B3D_HD int clz32(u32 x) {
 #ifdef __CUDA_ARCH__

@@ -1,0 +1,376 @@
+// Residue-number-system (RNS) multiprecision GEMM on the sm_100a INT8 tensor cores.
+//
+// C = A B for aligned operands (k_align: integer mantissas of at most NB = 32 L - 2 bits, a common exponent
+// per row of A and per column of B).  The exact integer product P = sum_k a b (|P| < K 2^(2 NB)) is computed
+// modulo n_p primes p_j < 2^31 whose product M exceeds 4 max |P|, then reconstructed by the Chinese remainder
+// theorem and rounded once: the result is bit-identical to the exact schoolbook product (k_gemm_aligned).
+//
+//   1. k_rns_split: each operand element -> its n_p residues, each cut into four 8-bit digits, written as
+//      unsigned int8 matrices in the canonical K-major UMMA layout (core matrices of 8 rows x 16 bytes).
+//      Row r of the operand becomes rows 4 r + s (digit s) of the digit matrix.
+//   2. k_rns_mma: per (prime, batch, tile) one CTA: both tiles land in shared memory by bulk async copies
+//      (cp.async.bulk, the TMA engine) on an mbarrier, one thread issues tcgen05.mma.kind::i8 over K into a
+//      TMEM accumulator (128 lanes x TN columns, int32), and the epilogue reads TMEM with tcgen05.ld and folds
+//      the 16 digit products of each output, sum_{s,t} D[4i+s][4l+t] 2^(8(s+t)), to a residue mod p_j.
+//   3. k_rns_crt: per output, y_j = r_j (M/p_j)^-1 mod p_j, q = round(sum_j y_j / p_j) (double precision: the
+//      fraction stays within 1/4 of an integer because |P| < M/4), P = sum_j y_j (M/p_j) - q M exactly in
+//      limbs, rounded to NB bits with the exponents of its row and column.
+//
+// Every spin-wait (mbarrier phases) has an iteration limit; on expiry the CTA records an error code in a
+// device flag, waits (bounded) for its own copies, frees its TMEM and returns.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "mp.cuh"
+
+namespace b3d {
+
+// number of primes and limbs of M for L-limb operands and inner dimension K <= 4096
+B3D_CX int rns_primes(int L) { return (2 * (32 * L - 2) + 12 + 2 + 30) / 31 + 1; }
+B3D_CX int rns_mlimbs(int L) { return (31 * rns_primes(L) + 31) / 32 + 1; }
+
+// per-L tables (device memory, filled by the host: blocksvibe_b200/rns.py)
+struct RnsTables {
+    const uint32_t* p;       // (np) primes
+    const uint64_t* mu;      // (np) floor(2^62 / p)
+    const uint32_t* w;       // (np, 8) 2^(8u) mod p, u < 7
+    const uint32_t* conv;    // (np, L) 2^(32k) mod p
+    const uint32_t* inv;     // (np) (M / p)^-1 mod p
+    const uint32_t* mj;      // (np, ML) M / p, little-endian limbs
+    const uint32_t* mfull;   // (ML) M
+    const double* rp;        // (np) 1 / p
+    int np, ml;
+};
+
+// x mod p for x < 2^62, Barrett with mu = floor(2^62 / p), 2^30 < p < 2^31
+// (the quotient estimate is at most 3 below the true quotient)
+__device__ __forceinline__ uint32_t barrett(uint64_t x, uint32_t p, uint64_t mu) {
+    uint64_t xq = x >> 30;                      // < 2^32
+    uint64_t qq = (xq * mu) >> 32;              // xq < 2^32, mu < 2^32: the product fits 64 bits
+    uint64_t r = x - qq * (uint64_t)p;
+#pragma unroll
+    for (int c = 0; c < 3; c++) r = r >= p ? r - p : r;
+    return (uint32_t)r;
+}
+
+// ------------------------------------------------------------------------------------------------
+// 1. digits.  Element (b, r, k) of a strided aligned operand (two's complement limb planes, plane stride
+// `plane`, element index b * sb + r * sr + k * sk) -> digits of its residues at rows 4 r + s, column k of the
+// K-major tiled matrix of (prime j, batch b): out + (j * nb + b) * mat_bytes, tiles of TR rows:
+//   byte(row, k) = ((row / TR) * (Kp / 16) + k / 16) * (TR * 16) + ((row % TR) / 8) * 128 + (row % 8) * 16 + k % 16
+// Threads cover the padded matrix (rows < Rp, k < Kp); padding is written as zero.
+__device__ __forceinline__ size_t tiled_offset(int64_t row, int64_t k, int TR, int64_t Kp) {
+    return (size_t)(((row / TR) * (Kp / 16) + k / 16) * (TR * 16) + ((row % TR) / 8) * 128 + (row % 8) * 16 + k % 16);
+}
+
+template <int L>
+__global__ void k_rns_split(const int32_t* __restrict__ m, int64_t plane, int64_t nb, int64_t R, int64_t K,
+                            int64_t sb, int64_t sr, int64_t sk, int64_t Rp, int64_t Kp, int TR, RnsTables tb,
+                            uint8_t* __restrict__ out, int64_t mat_bytes) {
+    int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t >= nb * Rp * Kp) return;
+    int64_t k = t % Kp, r = (t / Kp) % Rp, b = t / (Kp * Rp);
+    const int np = tb.np;
+    bool live = r < R && k < K;
+    u32 a[L];
+    bool neg = false;
+    if (live) {
+        neg = load_mag<L>(m, plane, b * sb + r * sr + k * sk, a);
+    } else {
+        zero(a);
+    }
+    bool nz = !is_zero(a);
+    for (int j = 0; j < np; j++) {
+        uint32_t res = 0;
+        if (nz) {
+            const uint32_t* c = tb.conv + (size_t)j * L;
+            uint64_t lo = 0, hi = 0;                 // sum of 16-bit halves times constants: < 2L 2^47
+#pragma unroll
+            for (int q = 0; q < L; q++) {
+                uint32_t cq = __ldg(c + q);
+                lo += (uint64_t)(a[q] & 0xFFFFu) * cq;
+                hi += (uint64_t)(a[q] >> 16) * cq;
+            }
+            uint32_t p = __ldg(tb.p + j);
+            uint64_t mu = __ldg(tb.mu + j);
+            uint32_t rh = barrett(hi, p, mu);
+            uint32_t rl = barrett(lo, p, mu);
+            res = barrett(((uint64_t)rh << 16) + rl, p, mu);
+            if (neg && res) res = p - res;
+        }
+        uint8_t* base = out + ((size_t)j * nb + b) * mat_bytes;
+#pragma unroll
+        for (int s = 0; s < 4; s++) base[tiled_offset(4 * r + s, k, TR, Kp)] = (uint8_t)(res >> (8 * s));
+    }
+}
+
+// ------------------------------------------------------------------------------------------------
+// 2. tensor-core product with the residue epilogue
+struct RnsMma {
+    const uint8_t* X;        // digit matrices of the lane-side operand: (np, nb, tilesX, 128 x Kp)
+    const uint8_t* Y;        // digit matrices of the column-side operand: (np, nb, tilesY, TN x Kp)
+    int64_t x_mat, y_mat;    // bytes per (prime, batch) matrix
+    int64_t nb, NI, NL;      // batch, rows of X (i), rows of Y (l)
+    int Kp, TN;              // padded K (multiple of 32, <= 256), column tile (multiple of 16, <= 256)
+    int64_t tiles_l;         // column tiles (grid: x = row tiles * tiles_l, y = batch, z = prime)
+    int64_t out_b, out_i, out_l;   // output strides (elements) for (b, i, l); prime stride = nb * out_b
+    uint32_t* out;           // residues (np, nb, ...)
+    int* err;                // device error flag (0 = ok)
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+
+// bounded wait for phase `parity` of an mbarrier; false on timeout
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint32_t limit) {
+    uint32_t addr = smem_u32(bar);
+    for (uint32_t it = 0; it < limit; it++) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred P;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 P, [%1], %2;\n\t"
+            "selp.b32 %0, 1, 0, P;\n\t}"
+            : "=r"(done) : "r"(addr), "r"(parity) : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+__device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 ::"r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar)) : "memory");
+}
+
+// K-major, no swizzle: core matrices of 8 rows x 16 bytes; lbo = byte stride between K chunks of 16 bytes,
+// sbo = byte stride between groups of 8 rows
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr >> 4) & 0x3FFF);
+    d |= (uint64_t)((lbo >> 4) & 0x3FFF) << 16;
+    d |= (uint64_t)((sbo >> 4) & 0x3FFF) << 32;
+    d |= (uint64_t)1 << 46;                      // descriptor version for sm_100
+    return d;                                    // base offset 0, lbo mode 0, layout SWIZZLE_NONE (0)
+}
+
+constexpr uint32_t kWaitLimit = 1u << 24;
+
+#ifdef B3D_RNS_MMA
+__global__ void __launch_bounds__(128, 1) k_rns_mma(RnsMma a, RnsTables tb) {
+    extern __shared__ __align__(128) uint8_t smem[];
+    __shared__ __align__(8) uint64_t bar_load, bar_mma;
+    __shared__ uint32_t tmem_base_sh;
+    __shared__ int fail_sh;
+
+    const int TN = a.TN, Kp = a.Kp;
+    const int64_t j = blockIdx.z, b = blockIdx.y;
+    const int64_t ti = blockIdx.x / a.tiles_l, tl = blockIdx.x % a.tiles_l;
+    uint8_t* sX = smem;
+    uint8_t* sY = smem + 128 * Kp;
+    const uint32_t xbytes = 128u * Kp, ybytes = (uint32_t)TN * Kp;
+    const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+    uint32_t ncols = 32;
+    while (ncols < (uint32_t)TN) ncols <<= 1;
+
+    if (threadIdx.x == 0) {
+        fail_sh = 0;
+        mbar_init(&bar_load, 1);
+        mbar_init(&bar_mma, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                     ::"r"(smem_u32(&tmem_base_sh)), "r"(ncols) : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = tmem_base_sh;
+
+    if (threadIdx.x == 0) {
+        const uint8_t* gx = a.X + (size_t)(j * a.nb + b) * a.x_mat + (size_t)ti * xbytes;
+        const uint8_t* gy = a.Y + (size_t)(j * a.nb + b) * a.y_mat + (size_t)tl * ybytes;
+        mbar_expect_tx(&bar_load, xbytes + ybytes);
+        bulk_copy_g2s(sX, gx, xbytes, &bar_load);
+        bulk_copy_g2s(sY, gy, ybytes, &bar_load);
+    }
+    bool ok = mbar_wait(&bar_load, 0, kWaitLimit);
+    if (!ok) atomicExch(&fail_sh, 1);
+    __syncthreads();
+    bool run = fail_sh == 0;
+
+    if (run && threadIdx.x == 0) {
+        // instruction descriptor: s32 accumulator, u8 x u8, both K-major, M = 128, N = TN
+        const uint32_t idesc = (2u << 4) | ((uint32_t)(TN >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+        const uint32_t ax = smem_u32(sX), ay = smem_u32(sY);
+        for (int kk = 0; kk < Kp / 32; kk++) {
+            uint64_t da = umma_desc(ax + kk * 2 * (128 * 16), 128 * 16, 128);
+            uint64_t db = umma_desc(ay + kk * 2 * (TN * 16), TN * 16, 128);
+            uint32_t acc = kk > 0 ? 1u : 0u;
+            asm volatile(
+                "{\n\t.reg .pred p;\n\t"
+                "setp.ne.b32 p, %4, 0;\n\t"
+                "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}"
+                ::"r"(tmem), "l"(da), "l"(db), "r"(idesc), "r"(acc) : "memory");
+        }
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                     ::"r"(smem_u32(&bar_mma)) : "memory");
+    }
+    if (run) {
+        ok = mbar_wait(&bar_mma, 0, kWaitLimit);
+        if (!ok) atomicExch(&fail_sh, 2);
+    }
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    __syncthreads();
+    run = run && fail_sh == 0;
+
+    if (run) {
+        // epilogue: lane row = 4 i + s, columns 4 l + t
+        const uint32_t p = __ldg(tb.p + j);
+        const uint64_t mu = __ldg(tb.mu + j);
+        uint32_t w[7];
+#pragma unroll
+        for (int u = 0; u < 7; u++) w[u] = __ldg(tb.w + j * 8 + u);
+        const int row = threadIdx.x;                 // TMEM lane
+        const int s = row & 3;
+        const int64_t i = ti * 32 + row / 4;
+        const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16);
+        for (int c0 = 0; c0 < TN; c0 += 16) {
+            uint32_t d[16];
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+                "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
+                : "=r"(d[0]), "=r"(d[1]), "=r"(d[2]), "=r"(d[3]), "=r"(d[4]), "=r"(d[5]), "=r"(d[6]), "=r"(d[7]),
+                  "=r"(d[8]), "=r"(d[9]), "=r"(d[10]), "=r"(d[11]), "=r"(d[12]), "=r"(d[13]), "=r"(d[14]), "=r"(d[15])
+                : "r"(taddr + (uint32_t)c0));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                uint64_t v = 0;
+#pragma unroll
+                for (int t = 0; t < 4; t++) v += (uint64_t)d[4 * q + t] * w[s + t];
+                v += __shfl_xor_sync(0xFFFFFFFFu, v, 1);
+                v += __shfl_xor_sync(0xFFFFFFFFu, v, 2);
+                const int64_t l = tl * (TN / 4) + c0 / 4 + q;
+                if (s == 0 && i < a.NI && l < a.NL) {
+                    uint32_t r = barrett(v, p, mu);
+                    a.out[(j * a.nb + b) * a.out_b + i * a.out_i + l * a.out_l] = r;
+                }
+            }
+        }
+    }
+    if (threadIdx.x == 0 && fail_sh) {              // bounded drain of our own copies and MMAs
+        if (!mbar_wait(&bar_load, 0, kWaitLimit)) fail_sh = 3;
+        else if (fail_sh == 2 && !mbar_wait(&bar_mma, 0, kWaitLimit)) fail_sh = 4;
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncols) : "memory");
+    }
+    if (threadIdx.x == 0 && fail_sh) atomicExch(a.err, fail_sh);
+}
+#endif
+
+// ------------------------------------------------------------------------------------------------
+// 3. reconstruction: residues (np, n) with element index e = b * sb_out ... -> normalised MPF
+template <int L>
+__global__ void k_rns_crt(const uint32_t* __restrict__ res, int64_t n, const int64_t* __restrict__ ea,
+                          const int64_t* __restrict__ eb, int64_t nbatch, int64_t M, int64_t N, RnsTables tb,
+                          int32_t* __restrict__ cm, int64_t* __restrict__ ce, int64_t cplane) {
+    constexpr int ML = rns_mlimbs(L);
+    constexpr int NA = ML + 1;
+    int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (e >= n) return;
+    int64_t col = e % N, row = (e / N) % M, b = e / (M * N);
+    int64_t Ea = ea[b * M + row], Eb = eb[b * N + col];
+    u32 acc[NA];
+    zero(acc);
+    double f = 0.0;
+    const int np = tb.np;
+    for (int jj = 0; jj < np; jj++) {
+        uint32_t r = res[(size_t)jj * n + e];
+        uint32_t p = __ldg(tb.p + jj);
+        uint64_t mu = __ldg(tb.mu + jj);
+        uint32_t y = barrett((uint64_t)r * __ldg(tb.inv + jj), p, mu);
+        f += (double)y * __ldg(tb.rp + jj);
+        // acc += y * (M / p_j)
+        const uint32_t* mj = tb.mj + (size_t)jj * ML;
+        uint32_t carry = 0;
+#pragma unroll
+        for (int c = 0; c < ML; c++) {
+            uint64_t v = (uint64_t)y * __ldg(mj + c) + acc[c] + carry;
+            acc[c] = (uint32_t)v;
+            carry = (uint32_t)(v >> 32);
+        }
+        acc[ML] += carry;
+    }
+    // subtract round(f) M: the result is the signed product in (-M/4, M/4)
+    uint32_t q = (uint32_t)llrint(f);
+    uint32_t borrow = 0;
+    {
+        uint32_t carry = 0;
+        u32 qm[NA];
+#pragma unroll
+        for (int c = 0; c < ML; c++) {
+            uint64_t v = (uint64_t)q * __ldg(tb.mfull + c) + carry;
+            qm[c] = (uint32_t)v;
+            carry = (uint32_t)(v >> 32);
+        }
+        qm[ML] = carry;
+#pragma unroll
+        for (int c = 0; c < NA; c++) {
+            uint64_t v = (uint64_t)acc[c] - qm[c] - borrow;
+            acc[c] = (uint32_t)v;
+            borrow = (uint32_t)(v >> 63);
+        }
+    }
+    bool zero_out = Ea == EZ || Eb == EZ;
+    if (zero_out) zero(acc);
+    store_rounded<L, NA>(cm, ce, cplane, e, acc, zero_out ? EZ : Ea + Eb);
+}
+
+}  // namespace b3d
+
+namespace b3d {
+
+// host-side launchers (instantiated per L in inst.cu; the MMA launcher lives in rns_mma.cu)
+template <int L>
+struct RnsLaunch {
+    static int split(const int32_t* m, int64_t plane, int64_t nb, int64_t R, int64_t K, int64_t sb, int64_t sr,
+                     int64_t sk, int64_t Rp, int64_t Kp, int TR, const RnsTables& tb, uint8_t* out,
+                     int64_t mat_bytes, cudaStream_t st);
+    static int crt(const uint32_t* res, int64_t n, const int64_t* ea, const int64_t* eb, int64_t nbatch, int64_t M,
+                   int64_t N, const RnsTables& tb, int32_t* cm, int64_t* ce, int64_t cplane, cudaStream_t st);
+};
+
+#ifdef B3D_DEFINE_LAUNCH
+template <int L>
+int RnsLaunch<L>::split(const int32_t* m, int64_t plane, int64_t nb, int64_t R, int64_t K, int64_t sb, int64_t sr,
+                        int64_t sk, int64_t Rp, int64_t Kp, int TR, const RnsTables& tb, uint8_t* out,
+                        int64_t mat_bytes, cudaStream_t st) {
+    int64_t n = nb * Rp * Kp;
+    if (n == 0) return 0;
+    k_rns_split<L><<<(unsigned)((n + 127) / 128), 128, 0, st>>>(m, plane, nb, R, K, sb, sr, sk, Rp, Kp, TR, tb, out, mat_bytes);
+    return (int)cudaGetLastError();
+}
+
+template <int L>
+int RnsLaunch<L>::crt(const uint32_t* res, int64_t n, const int64_t* ea, const int64_t* eb, int64_t nbatch, int64_t M,
+                      int64_t N, const RnsTables& tb, int32_t* cm, int64_t* ce, int64_t cplane, cudaStream_t st) {
+    if (n == 0) return 0;
+    k_rns_crt<L><<<(unsigned)((n + 127) / 128), 128, 0, st>>>(res, n, ea, eb, nbatch, M, N, tb, cm, ce, cplane);
+    return (int)cudaGetLastError();
+}
+#endif
+
+}  // namespace b3d

@@ -1,0 +1,21 @@
+// The tensor-core residue product (k_rns_mma) and its launcher: one translation unit, independent of L.
+#define B3D_RNS_MMA
+#include "abi_internal.h"
+
+namespace b3d {
+
+int rns_mma_launch(const RnsMma& a, const RnsTables& tb, cudaStream_t st) {
+    static bool configured = false;
+    const int smem = (128 + a.TN) * a.Kp;
+    if (!configured) {
+        int rc = (int)cudaFuncSetAttribute(k_rns_mma, cudaFuncAttributeMaxDynamicSharedMemorySize, (128 + 256) * 256);
+        if (rc) return rc;
+        configured = true;
+    }
+    const int64_t tiles_i = (4 * a.NI + 127) / 128;
+    dim3 grid((unsigned)(tiles_i * a.tiles_l), (unsigned)a.nb, (unsigned)tb.np);
+    k_rns_mma<<<grid, 128, smem, st>>>(a, tb);
+    return (int)cudaGetLastError();
+}
+
+}  // namespace b3d

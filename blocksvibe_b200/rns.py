@@ -1,0 +1,184 @@
+"""Host side of the residue-number-system GEMM (csrc/rns.cuh): prime tables per limb count and the three
+launches (digit split, tensor-core residue product, CRT).  ``gemm_rns(A, B)`` has the semantics of
+``mpf.gemm`` and returns the same bits as the schoolbook path: both compute the exact integer dot products
+of the aligned operands and round once."""
+import ctypes
+from math import prod
+
+import numpy as np
+import torch
+
+from . import _lib
+from .mpf import MPF, align_cols, align_rows
+
+_P = ctypes.c_void_p
+_I = ctypes.c_int
+_Q = ctypes.c_int64
+
+
+class RnsTables(ctypes.Structure):
+    _fields_ = [("p", _P), ("mu", _P), ("w", _P), ("conv", _P), ("inv", _P), ("mj", _P), ("mfull", _P),
+                ("rp", _P), ("np", _I), ("ml", _I)]
+
+
+class RnsMmaArgs(ctypes.Structure):
+    _fields_ = [("X", _P), ("Y", _P), ("x_mat", _Q), ("y_mat", _Q), ("nb", _Q), ("NI", _Q), ("NL", _Q),
+                ("Kp", _I), ("TN", _I), ("tiles_l", _Q), ("out_b", _Q), ("out_i", _Q), ("out_l", _Q),
+                ("out", _P), ("err", _P)]
+
+
+def _bind():
+    lib = _lib.lib()
+    if getattr(lib, "_rns_bound", False):
+        return lib
+    lib.b3d_rns_layout.argtypes = [_I, ctypes.POINTER(_I), ctypes.POINTER(_I)]
+    lib.b3d_rns_split.argtypes = [_I, _P, _Q, _Q, _Q, _Q, _Q, _Q, _Q, _Q, _Q, _I, ctypes.POINTER(RnsTables), _P, _Q, _P]
+    lib.b3d_rns_mma.argtypes = [ctypes.POINTER(RnsMmaArgs), ctypes.POINTER(RnsTables), _P]
+    lib.b3d_rns_crt.argtypes = [_I, _P, _Q, _P, _P, _Q, _Q, _Q, ctypes.POINTER(RnsTables), _P, _P, _Q, _P]
+    for f in (lib.b3d_rns_layout, lib.b3d_rns_split, lib.b3d_rns_mma, lib.b3d_rns_crt):
+        f.restype = _I
+    lib._rns_bound = True
+    return lib
+
+
+def _check(rc, name):
+    if rc != 0:
+        raise _lib.B3DError(f"{name} failed ({rc}): {_lib.lib().b3d_last_error().decode()}")
+
+
+def _is_prime(n):
+    """deterministic Miller-Rabin for n < 2^64"""
+    if n < 2:
+        return False
+    for p in (2, 3, 5, 7, 11, 13, 17, 19, 23, 29, 31, 37):
+        if n % p == 0:
+            return n == p
+    d, s = n - 1, 0
+    while d % 2 == 0:
+        d //= 2
+        s += 1
+    for a in (2, 3, 5, 7, 11, 13, 17, 19, 23, 29, 31, 37):
+        x = pow(a, d, n)
+        if x in (1, n - 1):
+            continue
+        for _ in range(s - 1):
+            x = x * x % n
+            if x == n - 1:
+                break
+        else:
+            return False
+    return True
+
+
+def primes_below_2_31(count):
+    out, n = [], (1 << 31) - 1
+    while len(out) < count:
+        if _is_prime(n):
+            out.append(n)
+        n -= 2
+    return out
+
+
+def layout(L):
+    lib = _bind()
+    np_, ml = _I(), _I()
+    _check(lib.b3d_rns_layout(L, ctypes.byref(np_), ctypes.byref(ml)), "b3d_rns_layout")
+    return np_.value, ml.value
+
+
+class Tables:
+    """constant tables for L-limb operands on one device"""
+
+    def __init__(self, L, device):
+        self.L = L
+        npr, ml = layout(L)
+        ps = primes_below_2_31(npr)
+        M = prod(ps)
+        NB = 32 * L - 2
+        assert M.bit_length() > 2 * NB + 12 + 2, "prime set too small"
+        assert M.bit_length() <= 32 * ml
+        limbs = lambda x, n: [(x >> (32 * i)) & 0xFFFFFFFF for i in range(n)]
+        mj = [M // p for p in ps]
+        t = lambda a, dt: torch.tensor(np.array(a, dtype=dt), device=device)
+        self.p = t(ps, np.uint32).view(torch.int32)
+        self.mu = t([(1 << 62) // p for p in ps], np.uint64).view(torch.int64)
+        self.w = t([[pow(2, 8 * u, p) for u in range(8)] for p in ps], np.uint32).view(torch.int32)
+        self.conv = t([[pow(2, 32 * k, p) for k in range(L)] for p in ps], np.uint32).view(torch.int32)
+        self.inv = t([pow(m % p, -1, p) for m, p in zip(mj, ps)], np.uint32).view(torch.int32)
+        self.mj = t([limbs(m, ml) for m in mj], np.uint32).view(torch.int32)
+        self.mfull = t(limbs(M, ml), np.uint32).view(torch.int32)
+        self.rp = t([1.0 / p for p in ps], np.float64)
+        self.np, self.ml = npr, ml
+        self.err = torch.zeros(1, dtype=torch.int32, device=device)
+        self.c = RnsTables(self.p.data_ptr(), self.mu.data_ptr(), self.w.data_ptr(), self.conv.data_ptr(),
+                           self.inv.data_ptr(), self.mj.data_ptr(), self.mfull.data_ptr(), self.rp.data_ptr(), npr, ml)
+
+
+_TABLES = {}
+
+
+def tables(L, device):
+    key = (L, str(device))
+    if key not in _TABLES:
+        _TABLES[key] = Tables(L, device)
+    return _TABLES[key]
+
+
+def _round_up(x, m):
+    return -(-x // m) * m
+
+
+def _split(tb, m, plane, nb, R, K, sb, sr, sk, Kp, TR, stream):
+    """digit matrices (np, nb, 4 Rp x Kp) of an aligned operand with R rows, tiles of TR digit rows"""
+    rows_per_tile = TR // 4
+    Rp = _round_up(max(R, 1), rows_per_tile)
+    mat = 4 * Rp * Kp
+    out = torch.empty(tb.np * nb * mat, dtype=torch.uint8, device=m.device)
+    _check(_bind().b3d_rns_split(tb.L, m.data_ptr(), plane, nb, R, K, sb, sr, sk, Rp, Kp, TR, ctypes.byref(tb.c),
+                                 out.data_ptr(), mat, stream), "b3d_rns_split")
+    return out, mat, Rp
+
+
+def gemm_aligned_rns(Aal, Bal):
+    """(row-aligned A (L, nb, M, K), (nb, M)) x (column-aligned B (L, nb, K, N), (nb, N)) -> MPF (nb, M, N),
+    on the tensor cores; K <= 256"""
+    am, ae = Aal
+    bm, be = Bal
+    L, nb, M, K = am.shape
+    N = bm.shape[-1]
+    dev = am.device
+    if K > 256:
+        raise ValueError("gemm_aligned_rns: K > 256")
+    tb = tables(L, dev)
+    stream = torch.cuda.current_stream(dev).cuda_stream
+    Kp = _round_up(max(K, 1), 32)
+    # the operand with more rows goes on the 128 TMEM lanes
+    a_rows = dict(m=am, plane=am.stride(0), R=M, sb=M * K, sr=K, sk=1)
+    b_rows = dict(m=bm, plane=bm.stride(0), R=N, sb=K * N, sr=1, sk=N)
+    if M >= N:
+        xs, ys, out_i, out_l = a_rows, b_rows, N, 1
+    else:
+        xs, ys, out_i, out_l = b_rows, a_rows, 1, N
+    NL = ys["R"]
+    TN = min(256, _round_up(4 * NL, 16))
+    X, x_mat, _ = _split(tb, xs["m"], xs["plane"], nb, xs["R"], K, xs["sb"], xs["sr"], xs["sk"], Kp, 128, stream)
+    Y, y_mat, Rp_y = _split(tb, ys["m"], ys["plane"], nb, NL, K, ys["sb"], ys["sr"], ys["sk"], Kp, TN, stream)
+    res = torch.empty(tb.np * nb * M * N, dtype=torch.int32, device=dev)
+    args = RnsMmaArgs(X.data_ptr(), Y.data_ptr(), x_mat, y_mat, nb, xs["R"], NL, Kp, TN, (4 * Rp_y) // TN,
+                      M * N, out_i, out_l, res.data_ptr(), tb.err.data_ptr())
+    _check(_bind().b3d_rns_mma(ctypes.byref(args), ctypes.byref(tb.c), stream), "b3d_rns_mma")
+    cm = torch.empty((L, nb * M * N), dtype=torch.int32, device=dev)
+    ce = torch.empty((nb, M, N), dtype=torch.int64, device=dev)
+    _check(_bind().b3d_rns_crt(L, res.data_ptr(), nb * M * N, ae.contiguous().data_ptr(), be.contiguous().data_ptr(),
+                               nb, M, N, ctypes.byref(tb.c), cm.data_ptr(), ce.data_ptr(), cm.stride(0), stream),
+           "b3d_rns_crt")
+    return MPF(cm.reshape(L, nb, M, N), ce)
+
+
+def check_errors(device):
+    """raise if a tensor-core launch on `device` recorded a timeout (bounded mbarrier waits)"""
+    for (L, dev), tb in _TABLES.items():
+        if dev == str(device) and int(tb.err.item()) != 0:
+            code = int(tb.err.item())
+            tb.err.zero_()
+            raise _lib.B3DError(f"b3d_rns_mma: a wait timed out (code {code})")

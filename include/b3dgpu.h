@@ -99,6 +99,53 @@ int b3d_moments_level(int L, const int32_t* rm, const int64_t* re, int64_t rplan
                       const int64_t* q_n, int64_t Q, int64_t N, int R1, int32_t* mm, int64_t* me, int64_t mplane,
                       void* stream);
 
+/* ---- residue-number-system GEMM on the INT8 tensor cores (tcgen05), the replacement of the reference's
+ * un-vendored sdpvibe mpf.gemm (RNS / INT8; called at recursion_gpu.py:53-79, derivatives.py:540-580,
+ * output.py:189,211).  Exact products, one rounding: bit-identical to b3d_gemm_aligned. */
+
+/* per-limb-count constant tables (device pointers; built by blocksvibe_b200/rns.py) */
+typedef struct b3d_rns_tables {
+    const uint32_t* p;       /* (np) primes, 2^30 < p < 2^31 */
+    const uint64_t* mu;      /* (np) floor(2^62 / p) */
+    const uint32_t* w;       /* (np, 8) 2^(8u) mod p */
+    const uint32_t* conv;    /* (np, L) 2^(32k) mod p */
+    const uint32_t* inv;     /* (np) (M / p)^-1 mod p */
+    const uint32_t* mj;      /* (np, ml) M / p, 32-bit limbs */
+    const uint32_t* mfull;   /* (ml) M */
+    const double* rp;        /* (np) 1 / p */
+    int np, ml;
+} b3d_rns_tables;
+
+/* primes and limbs of M the kernels for L limbs expect (K <= 4096) */
+int b3d_rns_layout(int L, int* np, int* ml);
+
+/* aligned operand (b3d_align output, element b * sb + r * sr + k * sk) -> int8 digit matrices of its residues,
+ * K-major UMMA core-matrix layout, tiles of TR digit rows, (np, nb, mat_bytes); rows padded to Rp, K to Kp */
+int b3d_rns_split(int L, const int32_t* m, int64_t plane, int64_t nb, int64_t R, int64_t K, int64_t sb, int64_t sr,
+                  int64_t sk, int64_t Rp, int64_t Kp, int TR, const b3d_rns_tables* tb, uint8_t* out,
+                  int64_t mat_bytes, void* stream);
+
+typedef struct b3d_rns_mma_args {
+    const uint8_t* X;        /* lane-side digit matrices (tiles of 128 digit rows) */
+    const uint8_t* Y;        /* column-side digit matrices (tiles of TN digit rows) */
+    int64_t x_mat, y_mat;    /* bytes per (prime, batch) matrix */
+    int64_t nb, NI, NL;      /* batch, operand rows of X and of Y */
+    int Kp, TN;              /* padded K (multiple of 32, <= 256), column tile (multiple of 16, <= 256) */
+    int64_t tiles_l;         /* column tiles */
+    int64_t out_b, out_i, out_l;   /* residue output strides (elements) */
+    uint32_t* out;           /* (np, nb, ...) residues */
+    int* err;                /* device error flag, 0 = ok */
+} b3d_rns_mma_args;
+
+/* residues of X Y^T per prime with tcgen05.mma.kind::i8 (TMEM accumulators, bulk async copies) */
+int b3d_rns_mma(const b3d_rns_mma_args* args, const b3d_rns_tables* tb, void* stream);
+
+/* CRT reconstruction of (np, n) residues, element e = (b * M + i) * N + l, rounded with exponents
+ * ea[b * M + i] + eb[b * N + l] -> normalised MPF C (n) */
+int b3d_rns_crt(int L, const uint32_t* res, int64_t n, const int64_t* ea, const int64_t* eb, int64_t nbatch,
+                int64_t M, int64_t N, const b3d_rns_tables* tb, int32_t* cm, int64_t* ce, int64_t cplane,
+                void* stream);
+
 /* Size of the device scratch array of b3d_pole_level_noalloc (per GPU, held until the process exits). */
 #define B3D_NOALLOC_SCRATCH_BYTES ((size_t)16 << 20)
 

@@ -1,0 +1,49 @@
+"""The tensor-core RNS GEMM (tcgen05.mma.kind::i8 on residues, CRT) against the exact schoolbook GEMM on the
+CUDA cores: both compute the exact integer dot products of the aligned operands and round once, so the
+results must be identical bit for bit, for any shape, batch, sign pattern and limb count."""
+import pytest
+import torch
+
+from blocksvibe_b200 import mpf, rns
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("L,nb,M,K,N", [
+    (10, 1, 4, 3, 5),          # tiny, padded everywhere
+    (10, 3, 40, 33, 70),       # M < N: B on the TMEM lanes
+    (10, 2, 130, 64, 17),      # several row tiles
+    (18, 1, 12, 98, 600),      # numerator-like
+    (34, 1, 42, 42, 300),      # write_output-like, 1024 bits
+    (34, 5, 12, 12, 50),       # residues a_i[e]-like batch
+    (42, 1, 66, 192, 96),      # 1280 bits, K near the limit
+    (10, 1, 3, 256, 260),      # K = 256, N > one column tile
+])
+def test_rns_gemm_bitwise_equals_schoolbook(cuda, L, nb, M, K, N):
+    g = torch.Generator().manual_seed(L * 1000 + M + K + N)
+    A = mpf.random_mpf((nb, M, K), L, spread=20, device=cuda, generator=g)
+    B = mpf.random_mpf((nb, K, N), L, spread=20, device=cuda, generator=g)
+    # zeros and exact cancellations
+    A.m[:, 0, 0, 0] = 0
+    A.e[0, 0, 0] = mpf.EZ
+    Aal, Bal = mpf.align_rows(A), mpf.align_cols(B)
+    ref = mpf.gemm_aligned(Aal, Bal)
+    got = rns.gemm_aligned_rns(Aal, Bal)
+    torch.cuda.synchronize()
+    rns.check_errors(cuda)
+    assert torch.equal(ref.e, got.e)
+    assert torch.equal(ref.m, got.m)
+
+
+def test_rns_gemm_cancellation(cuda):
+    """rows that cancel exactly give zero; nearly cancelling sums keep all their bits"""
+    L = 10
+    g = torch.Generator().manual_seed(5)
+    A = mpf.random_mpf((1, 2, 8), L, spread=4, device=cuda, generator=g)
+    B = mpf.random_mpf((1, 8, 3), L, spread=4, device=cuda, generator=g)
+    A.m[:, 0, 1, :] = A.m[:, 0, 0, :]                  # row 1 = row 0: rows give equal results
+    A.e[0, 1, :] = A.e[0, 0, :]
+    Aal, Bal = mpf.align_rows(A), mpf.align_cols(B)
+    ref = mpf.gemm_aligned(Aal, Bal)
+    got = rns.gemm_aligned_rns(Aal, Bal)
+    assert torch.equal(ref.m, got.m) and torch.equal(ref.e, got.e)
