@@ -244,8 +244,7 @@ def run_ours(args):
 
     def step_e2e():
         nums = run([t], ns)
-        outs = op.apply_outputs(nums, t.delta_1_plus_2)
-        host = {k: (r.m.cpu(), r.e.cpu()) for k, r in outs.items()}
+        host = op.to_host(op.apply_outputs(nums, t.delta_1_plus_2))
         d2h[0] = sum(m.numel() * 4 + e.numel() * 8 for m, e in host.values())
         return host
 
@@ -281,6 +280,19 @@ def run_ours(args):
     probe.watch = None
     clk = clocks.stop(local) if rank == 0 else None
     ms = max_over_ranks(ms, world, dev)
+
+    # the other schedule, same timing, for the batched-vs-plain comparison
+    other = op.run_plain if args.schedule == "batched" else op.run_batched
+    for _ in range(2):
+        op.apply_outputs(other([dtask], ns), t.delta_1_plus_2)
+    torch.cuda.synchronize()
+    s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s0.record()
+    for _ in range(args.steps):
+        op.apply_outputs(other([dtask], ns), t.delta_1_plus_2)
+    s1.record()
+    torch.cuda.synchronize()
+    other_ms = max_over_ranks(s0.elapsed_time(s1) / args.steps, world, dev)
 
     # end to end through the host interface, per-step latencies for p50 / p99
     for _ in range(args.warmup):
@@ -338,6 +350,8 @@ def run_ours(args):
             "e2e": {"value": world / e2e_s, "unit": "tasks/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h[0]},
             "latency_ms": {"p50": pct(0.5), "p99": pct(0.99), "source": "e2e steps"},
             "gpu_launches": launches, "setup_s": t_setup,
+            "other_schedule": {"schedule": "plain" if args.schedule == "batched" else "batched",
+                               "value": world / (other_ms / 1e3), "ms_per_step": other_ms},
             "kernel_split_ms": {k: round(v, 3) for k, v in sorted(split.items(), key=lambda x: -x[1])},
             "roofline": roof, "cpu_baseline": cpu, "clocks": clk}
     print(json.dumps(line), flush=True)

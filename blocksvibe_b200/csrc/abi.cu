@@ -140,9 +140,21 @@ int b3d_rns_mma(const b3d_rns_mma_args* a, const b3d_rns_tables* tb, void* strea
         a->y_mat < a->tiles_l * a->TN * (int64_t)a->Kp)
         return fail(B3D_E_ARG, "b3d_rns_mma: invalid sizes");
     if (a->NI == 0 || a->NL == 0) return 0;
+    if (a->yb && (a->crt_kp % 32 || a->crt_kp < 4 * (int64_t)tb->np))
+        return fail(B3D_E_ARG, "b3d_rns_mma: CRT operand row too short");
     b3d::RnsMma m{a->X, a->Y, a->x_mat, a->y_mat, a->nb, a->NI, a->NL, a->Kp, a->TN, a->tiles_l, a->out_b, a->out_i,
-                  a->out_l, a->out, a->err};
+                  a->out_l, a->out, a->err, a->yb, a->crt_kp};
     return cuda_status(b3d::rns_mma_launch(m, tables_of(tb), as_stream(stream)), "b3d_rns_mma");
+}
+
+int b3d_rns_crt_mma(int L, const b3d_rns_crt_args* a, const b3d_rns_tables* tb, void* stream) {
+    if (!a || !tb || tb->np != b3d::rns_primes(L) || tb->ml != b3d::rns_mlimbs(L) || a->Kc % 32 ||
+        a->Kc < 4 * tb->np || a->NH % 16 || a->NH <= 0 || a->NH > 256 || 2 * a->NH < 4 * tb->ml + 3 ||
+        (128 + 2 * a->NH) * a->Kc > 200 * 1024 || a->n != a->nbatch * a->M * a->N || a->n < 0)
+        return fail(B3D_E_ARG, "b3d_rns_crt_mma: invalid sizes or tables");
+    b3d::RnsCrt c{a->A, a->T, a->Kc, a->NH, a->n, a->nbatch, a->M, a->N, a->ea, a->eb, a->cm, a->ce, a->cplane, a->err};
+    b3d::RnsTables t = tables_of(tb);
+    B3D_DISPATCH_RNS(L, cuda_status(RX::crt_mma(c, t, as_stream(stream)), "b3d_rns_crt_mma"));
 }
 
 int b3d_rns_crt(int L, const uint32_t* res, int64_t n, const int64_t* ea, const int64_t* eb, int64_t nbatch,

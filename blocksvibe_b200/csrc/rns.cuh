@@ -64,43 +64,55 @@ __device__ __forceinline__ size_t tiled_offset(int64_t row, int64_t k, int TR, i
 }
 
 template <int L>
+__device__ __forceinline__ uint32_t residue_of(const u32 (&a)[L], bool neg, const RnsTables& tb, int j) {
+    const uint32_t* c = tb.conv + (size_t)j * L;
+    uint64_t lo = 0, hi = 0;                     // sums of 16-bit halves times constants: < 2 L 2^47
+#pragma unroll
+    for (int q = 0; q < L; q++) {
+        uint32_t cq = __ldg(c + q);
+        lo += (uint64_t)(a[q] & 0xFFFFu) * cq;
+        hi += (uint64_t)(a[q] >> 16) * cq;
+    }
+    uint32_t p = __ldg(tb.p + j);
+    uint64_t mu = __ldg(tb.mu + j);
+    uint32_t r = barrett(((uint64_t)barrett(hi, p, mu) << 16) + barrett(lo, p, mu), p, mu);
+    return (neg && r) ? p - r : r;
+}
+
+// threads cover (b, r < Rp, k4 < Kp / 4): four consecutive k of one row, one 32-bit store per (prime, digit)
+template <int L>
 __global__ void k_rns_split(const int32_t* __restrict__ m, int64_t plane, int64_t nb, int64_t R, int64_t K,
                             int64_t sb, int64_t sr, int64_t sk, int64_t Rp, int64_t Kp, int TR, RnsTables tb,
                             uint8_t* __restrict__ out, int64_t mat_bytes) {
     int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (t >= nb * Rp * Kp) return;
-    int64_t k = t % Kp, r = (t / Kp) % Rp, b = t / (Kp * Rp);
+    const int64_t K4 = Kp / 4;
+    if (t >= nb * Rp * K4) return;
+    int64_t k0 = (t % K4) * 4, r = (t / K4) % Rp, b = t / (K4 * Rp);
     const int np = tb.np;
-    bool live = r < R && k < K;
-    u32 a[L];
-    bool neg = false;
-    if (live) {
-        neg = load_mag<L>(m, plane, b * sb + r * sr + k * sk, a);
-    } else {
-        zero(a);
-    }
-    bool nz = !is_zero(a);
-    for (int j = 0; j < np; j++) {
-        uint32_t res = 0;
-        if (nz) {
-            const uint32_t* c = tb.conv + (size_t)j * L;
-            uint64_t lo = 0, hi = 0;                 // sum of 16-bit halves times constants: < 2L 2^47
+    u32 a[4][L];
+    bool neg[4], nz[4];
 #pragma unroll
-            for (int q = 0; q < L; q++) {
-                uint32_t cq = __ldg(c + q);
-                lo += (uint64_t)(a[q] & 0xFFFFu) * cq;
-                hi += (uint64_t)(a[q] >> 16) * cq;
-            }
-            uint32_t p = __ldg(tb.p + j);
-            uint64_t mu = __ldg(tb.mu + j);
-            uint32_t rh = barrett(hi, p, mu);
-            uint32_t rl = barrett(lo, p, mu);
-            res = barrett(((uint64_t)rh << 16) + rl, p, mu);
-            if (neg && res) res = p - res;
+    for (int u = 0; u < 4; u++) {
+        int64_t k = k0 + u;
+        if (r < R && k < K) {
+            neg[u] = load_mag<L>(m, plane, b * sb + r * sr + k * sk, a[u]);
+        } else {
+            zero(a[u]);
+            neg[u] = false;
         }
+        nz[u] = !is_zero(a[u]);
+    }
+    for (int j = 0; j < np; j++) {
+        uint32_t res[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) res[u] = nz[u] ? residue_of<L>(a[u], neg[u], tb, j) : 0u;
         uint8_t* base = out + ((size_t)j * nb + b) * mat_bytes;
 #pragma unroll
-        for (int s = 0; s < 4; s++) base[tiled_offset(4 * r + s, k, TR, Kp)] = (uint8_t)(res >> (8 * s));
+        for (int s = 0; s < 4; s++) {
+            uint32_t w = ((res[0] >> (8 * s)) & 0xFFu) | (((res[1] >> (8 * s)) & 0xFFu) << 8) |
+                         (((res[2] >> (8 * s)) & 0xFFu) << 16) | (((res[3] >> (8 * s)) & 0xFFu) << 24);
+            *reinterpret_cast<uint32_t*>(base + tiled_offset(4 * r + s, k0, TR, Kp)) = w;
+        }
     }
 }
 
@@ -114,8 +126,10 @@ struct RnsMma {
     int Kp, TN;              // padded K (multiple of 32, <= 256), column tile (multiple of 16, <= 256)
     int64_t tiles_l;         // column tiles (grid: x = row tiles * tiles_l, y = batch, z = prime)
     int64_t out_b, out_i, out_l;   // output strides (elements) for (b, i, l); prime stride = nb * out_b
-    uint32_t* out;           // residues (np, nb, ...)
+    uint32_t* out;           // residues (np, nb, ...), when yb is null
     int* err;                // device error flag (0 = ok)
+    uint8_t* yb;             // else: y_j = r_j (M/p_j)^-1 mod p_j as 4 bytes at row e, column 4 j of the CRT operand
+    int64_t crt_kp;          // bytes per row of the CRT operand (tiles of 128 rows)
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -237,6 +251,7 @@ __global__ void __launch_bounds__(128, 1) k_rns_mma(RnsMma a, RnsTables tb) {
         // epilogue: lane row = 4 i + s, columns 4 l + t
         const uint32_t p = __ldg(tb.p + j);
         const uint64_t mu = __ldg(tb.mu + j);
+        const uint32_t inv = __ldg(tb.inv + j);
         uint32_t w[7];
 #pragma unroll
         for (int u = 0; u < 7; u++) w[u] = __ldg(tb.w + j * 8 + u);
@@ -263,12 +278,165 @@ __global__ void __launch_bounds__(128, 1) k_rns_mma(RnsMma a, RnsTables tb) {
                 const int64_t l = tl * (TN / 4) + c0 / 4 + q;
                 if (s == 0 && i < a.NI && l < a.NL) {
                     uint32_t r = barrett(v, p, mu);
-                    a.out[(j * a.nb + b) * a.out_b + i * a.out_i + l * a.out_l] = r;
+                    const int64_t e = b * a.out_b + i * a.out_i + l * a.out_l;
+                    if (a.yb) {
+                        uint32_t y = barrett((uint64_t)r * inv, p, mu);
+                        *reinterpret_cast<uint32_t*>(a.yb + tiled_offset(e, 4 * j, 128, a.crt_kp)) = y;
+                    } else {
+                        a.out[j * a.nb * a.out_b + e] = r;
+                    }
                 }
             }
         }
     }
     if (threadIdx.x == 0 && fail_sh) {              // bounded drain of our own copies and MMAs
+        if (!mbar_wait(&bar_load, 0, kWaitLimit)) fail_sh = 3;
+        else if (fail_sh == 2 && !mbar_wait(&bar_mma, 0, kWaitLimit)) fail_sh = 4;
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncols) : "memory");
+    }
+    if (threadIdx.x == 0 && fail_sh) atomicExch(a.err, fail_sh);
+}
+#endif
+
+// ------------------------------------------------------------------------------------------------
+// 3'. CRT on the tensor cores.  A = the y bytes of 128 outputs (rows e, K = 4 np bytes, from k_rns_mma),
+// B = the constant matrix T[pos][4 j + a] = byte (pos - a) of M / p_j (two tiles of NH rows), so that
+// S[e][pos] = sum_{j,a} y_{j,a}(e) T[pos][4 j + a] and x' = sum_pos S[pos] 2^(8 pos) = sum_j y_j M / p_j
+// exactly (S < 4 np 255^2 < 2^25).  The epilogue thread of output e carries S into limbs, subtracts
+// round(x' / M) M (from the top limbs, in double precision) and rounds once to NB bits.
+struct RnsCrt {
+    const uint8_t* A;        // (tiles, 128 x Kc) y bytes
+    const uint8_t* T;        // (2 NH x Kc) constant Toeplitz digits, tiles of NH rows
+    int Kc, NH;              // K bytes (multiple of 32), half of the position count (multiple of 16)
+    int64_t n, nbatch, M, N; // outputs, their (b, row, col) shape
+    const int64_t* ea;       // (nbatch, M) row exponents
+    const int64_t* eb;       // (nbatch, N) column exponents
+    int32_t* cm;             // result limb planes
+    int64_t* ce;             // result exponents
+    int64_t cplane;
+    int* err;
+};
+
+#ifdef B3D_DEFINE_LAUNCH
+template <int L>
+__global__ void __launch_bounds__(128, 1) k_rns_crt_mma(RnsCrt a, RnsTables tb) {
+    constexpr int ML = rns_mlimbs(L);
+    constexpr int NX = ML + 2;
+    constexpr int NCH = (4 * ML + 3 + 15) / 16;      // 16-column chunks holding all positions
+    extern __shared__ __align__(128) uint8_t smem[];
+    __shared__ __align__(8) uint64_t bar_load, bar_mma;
+    __shared__ uint32_t tmem_base_sh;
+    __shared__ int fail_sh;
+    const int Kc = a.Kc, NH = a.NH;
+    uint8_t* sA = smem;
+    uint8_t* sT = smem + 128 * Kc;
+    const uint32_t abytes = 128u * Kc, tbytes = 2u * NH * Kc;
+    const int warp = threadIdx.x / 32;
+    const uint32_t ncols = 512;
+    if (threadIdx.x == 0) {
+        fail_sh = 0;
+        mbar_init(&bar_load, 1);
+        mbar_init(&bar_mma, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                     ::"r"(smem_u32(&tmem_base_sh)), "r"(ncols) : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = tmem_base_sh;
+    if (threadIdx.x == 0) {
+        mbar_expect_tx(&bar_load, abytes + tbytes);
+        bulk_copy_g2s(sA, a.A + (size_t)blockIdx.x * abytes, abytes, &bar_load);
+        bulk_copy_g2s(sT, a.T, tbytes, &bar_load);
+    }
+    if (!mbar_wait(&bar_load, 0, kWaitLimit)) atomicExch(&fail_sh, 1);
+    __syncthreads();
+    bool run = fail_sh == 0;
+    if (run && threadIdx.x == 0) {
+        const uint32_t idesc = (2u << 4) | ((uint32_t)(NH >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+        const uint32_t aa = smem_u32(sA), at = smem_u32(sT);
+        for (int h = 0; h < 2; h++) {
+            for (int kk = 0; kk < Kc / 32; kk++) {
+                uint64_t da = umma_desc(aa + kk * 2 * (128 * 16), 128 * 16, 128);
+                uint64_t db = umma_desc(at + h * NH * Kc + kk * 2 * (NH * 16), NH * 16, 128);
+                uint32_t acc = kk > 0 ? 1u : 0u;
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\t"
+                    "setp.ne.b32 p, %4, 0;\n\t"
+                    "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}"
+                    ::"r"(tmem + (uint32_t)(h * NH)), "l"(da), "l"(db), "r"(idesc), "r"(acc) : "memory");
+            }
+        }
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                     ::"r"(smem_u32(&bar_mma)) : "memory");
+    }
+    if (run && !mbar_wait(&bar_mma, 0, kWaitLimit)) atomicExch(&fail_sh, 2);
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    __syncthreads();
+    run = run && fail_sh == 0;
+    const int64_t e = (int64_t)blockIdx.x * 128 + threadIdx.x;
+    if (run) {
+        const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16);
+        u32 x[NX];
+        uint64_t carry = 0;
+#pragma unroll
+        for (int ch = 0; ch < NCH; ch++) {
+            uint32_t d[16];
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+                "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
+                : "=r"(d[0]), "=r"(d[1]), "=r"(d[2]), "=r"(d[3]), "=r"(d[4]), "=r"(d[5]), "=r"(d[6]), "=r"(d[7]),
+                  "=r"(d[8]), "=r"(d[9]), "=r"(d[10]), "=r"(d[11]), "=r"(d[12]), "=r"(d[13]), "=r"(d[14]), "=r"(d[15])
+                : "r"(taddr + (uint32_t)(16 * ch)));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                const int c = 4 * ch + q;
+                uint64_t v = carry + (uint64_t)d[4 * q] + ((uint64_t)d[4 * q + 1] << 8) +
+                             ((uint64_t)d[4 * q + 2] << 16) + ((uint64_t)d[4 * q + 3] << 24);
+                if (c < NX) x[c] = (uint32_t)v;
+                carry = v >> 32;
+            }
+        }
+#pragma unroll
+        for (int c = 4 * NCH; c < NX; c++) {
+            x[c] = (uint32_t)carry;
+            carry >>= 32;
+        }
+        // q = round(x' / M) from the top limbs
+        double xt = 0.0, mt = 0.0;
+#pragma unroll
+        for (int c = NX - 1; c >= ML - 4; c--) xt = xt * 4294967296.0 + (double)x[c];
+#pragma unroll
+        for (int c = ML - 1; c >= ML - 4; c--) mt = mt * 4294967296.0 + (double)__ldg(tb.mfull + c);
+        const uint32_t q = (uint32_t)llrint(xt / mt);
+        uint32_t mc = 0;
+        uint64_t borrow = 0;
+#pragma unroll
+        for (int c = 0; c < NX; c++) {
+            uint64_t prod = (c < ML ? (uint64_t)q * __ldg(tb.mfull + c) : 0) + mc;
+            mc = (uint32_t)(prod >> 32);
+            uint64_t v = (uint64_t)x[c] - (uint32_t)prod - borrow;
+            x[c] = (uint32_t)v;
+            borrow = v >> 63;
+        }
+        if (e < a.n) {
+            const int64_t col = e % a.N, row = (e / a.N) % a.M, b = e / (a.M * a.N);
+            const int64_t Ea = a.ea[b * a.M + row], Eb = a.eb[b * a.N + col];
+            const bool z = Ea == EZ || Eb == EZ;
+            if (z) zero(x);
+            store_rounded<L, NX>(a.cm, a.ce, a.cplane, e, x, z ? EZ : Ea + Eb);
+        }
+    }
+    if (threadIdx.x == 0 && fail_sh) {
         if (!mbar_wait(&bar_load, 0, kWaitLimit)) fail_sh = 3;
         else if (fail_sh == 2 && !mbar_wait(&bar_mma, 0, kWaitLimit)) fail_sh = 4;
     }
@@ -351,6 +519,7 @@ struct RnsLaunch {
                      int64_t mat_bytes, cudaStream_t st);
     static int crt(const uint32_t* res, int64_t n, const int64_t* ea, const int64_t* eb, int64_t nbatch, int64_t M,
                    int64_t N, const RnsTables& tb, int32_t* cm, int64_t* ce, int64_t cplane, cudaStream_t st);
+    static int crt_mma(const RnsCrt& a, const RnsTables& tb, cudaStream_t st);
 };
 
 #ifdef B3D_DEFINE_LAUNCH
@@ -358,7 +527,7 @@ template <int L>
 int RnsLaunch<L>::split(const int32_t* m, int64_t plane, int64_t nb, int64_t R, int64_t K, int64_t sb, int64_t sr,
                         int64_t sk, int64_t Rp, int64_t Kp, int TR, const RnsTables& tb, uint8_t* out,
                         int64_t mat_bytes, cudaStream_t st) {
-    int64_t n = nb * Rp * Kp;
+    int64_t n = nb * Rp * (Kp / 4);
     if (n == 0) return 0;
     k_rns_split<L><<<(unsigned)((n + 127) / 128), 128, 0, st>>>(m, plane, nb, R, K, sb, sr, sk, Rp, Kp, TR, tb, out, mat_bytes);
     return (int)cudaGetLastError();
@@ -369,6 +538,20 @@ int RnsLaunch<L>::crt(const uint32_t* res, int64_t n, const int64_t* ea, const i
                       int64_t N, const RnsTables& tb, int32_t* cm, int64_t* ce, int64_t cplane, cudaStream_t st) {
     if (n == 0) return 0;
     k_rns_crt<L><<<(unsigned)((n + 127) / 128), 128, 0, st>>>(res, n, ea, eb, nbatch, M, N, tb, cm, ce, cplane);
+    return (int)cudaGetLastError();
+}
+
+template <int L>
+int RnsLaunch<L>::crt_mma(const RnsCrt& a, const RnsTables& tb, cudaStream_t st) {
+    static bool configured = false;
+    const int smem = (128 + 2 * a.NH) * a.Kc;
+    if (!configured) {
+        int rc = (int)cudaFuncSetAttribute(k_rns_crt_mma<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        if (rc) return rc;
+        configured = true;
+    }
+    if (a.n == 0) return 0;
+    k_rns_crt_mma<L><<<(unsigned)((a.n + 127) / 128), 128, smem, st>>>(a, tb);
     return (int)cudaGetLastError();
 }
 #endif

@@ -127,6 +127,23 @@ class Operator:
     def apply_outputs(self, nums, d12):
         return {c: apply_per_order(o, nums) for (c, dd), o in self.outs.items() if dd == d12}
 
+    def to_host(self, outs):
+        """device results -> host limb arrays through reusable pinned buffers (one D2H copy per array)"""
+        host = {}
+        for c, r in outs.items():
+            key = (c, tuple(r.m.shape))
+            buf = getattr(self, "_pinned", {}).get(key)
+            if buf is None:
+                buf = (torch.empty(r.m.shape, dtype=torch.int32, pin_memory=True),
+                       torch.empty(r.e.shape, dtype=torch.int64, pin_memory=True))
+                self._pinned = getattr(self, "_pinned", {})
+                self._pinned[key] = buf
+            buf[0].copy_(r.m, non_blocking=True)
+            buf[1].copy_(r.e, non_blocking=True)
+            host[c] = buf
+        torch.cuda.current_stream(self.device).synchronize()
+        return host
+
 
 def run_group(group, tasks, M, device="cuda", schedule="batched", max_rhs=None):
     """All tasks of one group on the GPU.  M: matrices for the plan's keys (dict of decimal strings or an MPF
@@ -149,8 +166,8 @@ def run_group(group, tasks, M, device="cuda", schedule="batched", max_rhs=None):
             nums = op.run_batched(ch, ns) if schedule == "batched" else op.run_plain(ch, ns)
             vals = {}
             for d12 in d12s:
-                for c, r in op.apply_outputs(nums, d12).items():          # (Jo, 2, S2, nq, outputs, Dmax)
-                    vals[(c, d12)] = (r.m.cpu().numpy(), r.e.cpu().numpy())
+                for c, (m, e) in op.to_host(op.apply_outputs(nums, d12)).items():   # (Jo, 2, S2, nq, outputs, Dmax)
+                    vals[(c, d12)] = (m.numpy().copy(), e.numpy().copy())
             for q, t in enumerate(ch):
                 results[(tuple(t.q4), t.sign)] = (
                     tjs, pp, {k: (m[:, :, :, :, q], e[:, :, :, q]) for k, (m, e) in vals.items()},

@@ -254,6 +254,18 @@ def gemm_aligned(Aal, Bal):
     return MPF(cm.reshape(L, nb, M, N), ce)
 
 
+# GEMM backend: "auto" (tensor-core RNS GEMM for 8 <= K <= 256, the CUDA-core schoolbook GEMM otherwise),
+# "rns" or "schoolbook" (both give the same bits: exact dot products, one rounding)
+GEMM_BACKEND = "auto"
+RNS_MIN_K = 64
+
+
+def _use_rns(K):
+    if GEMM_BACKEND == "schoolbook" or K > 256:
+        return False
+    return GEMM_BACKEND == "rns" or K >= RNS_MIN_K
+
+
 def gemm(A, B, aidx=None):
     """multiprecision (batched) product with the semantics of the reference's mpf.gemm (A aligned per row,
     B per column, exact products, one rounding per entry; reference ``recursion_gpu.py:53-79``).
@@ -270,7 +282,12 @@ def gemm(A, B, aidx=None):
             Aal = (Aal[0].expand(-1, nb, -1, -1).contiguous(), Aal[1].expand(nb, -1).contiguous())
     else:
         Aal = align_rows(A)
-    C = gemm_aligned(Aal, align_cols(Bb))
+    Bal = align_cols(Bb)
+    if _use_rns(Aal[0].shape[-1]):
+        from .rns import gemm_aligned_rns
+        C = gemm_aligned_rns(Aal, Bal)
+    else:
+        C = gemm_aligned(Aal, Bal)
     return C if batched else C.reshape(*C.shape[1:])
 
 

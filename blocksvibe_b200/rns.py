@@ -24,7 +24,12 @@ class RnsTables(ctypes.Structure):
 class RnsMmaArgs(ctypes.Structure):
     _fields_ = [("X", _P), ("Y", _P), ("x_mat", _Q), ("y_mat", _Q), ("nb", _Q), ("NI", _Q), ("NL", _Q),
                 ("Kp", _I), ("TN", _I), ("tiles_l", _Q), ("out_b", _Q), ("out_i", _Q), ("out_l", _Q),
-                ("out", _P), ("err", _P)]
+                ("out", _P), ("err", _P), ("yb", _P), ("crt_kp", _Q)]
+
+
+class RnsCrtArgs(ctypes.Structure):
+    _fields_ = [("A", _P), ("T", _P), ("Kc", _I), ("NH", _I), ("n", _Q), ("nbatch", _Q), ("M", _Q), ("N", _Q),
+                ("ea", _P), ("eb", _P), ("cm", _P), ("ce", _P), ("cplane", _Q), ("err", _P)]
 
 
 def _bind():
@@ -35,7 +40,8 @@ def _bind():
     lib.b3d_rns_split.argtypes = [_I, _P, _Q, _Q, _Q, _Q, _Q, _Q, _Q, _Q, _Q, _I, ctypes.POINTER(RnsTables), _P, _Q, _P]
     lib.b3d_rns_mma.argtypes = [ctypes.POINTER(RnsMmaArgs), ctypes.POINTER(RnsTables), _P]
     lib.b3d_rns_crt.argtypes = [_I, _P, _Q, _P, _P, _Q, _Q, _Q, ctypes.POINTER(RnsTables), _P, _P, _Q, _P]
-    for f in (lib.b3d_rns_layout, lib.b3d_rns_split, lib.b3d_rns_mma, lib.b3d_rns_crt):
+    lib.b3d_rns_crt_mma.argtypes = [_I, ctypes.POINTER(RnsCrtArgs), ctypes.POINTER(RnsTables), _P]
+    for f in (lib.b3d_rns_layout, lib.b3d_rns_split, lib.b3d_rns_mma, lib.b3d_rns_crt, lib.b3d_rns_crt_mma):
         f.restype = _I
     lib._rns_bound = True
     return lib
@@ -110,6 +116,18 @@ class Tables:
         self.rp = t([1.0 / p for p in ps], np.float64)
         self.np, self.ml = npr, ml
         self.err = torch.zeros(1, dtype=torch.int32, device=device)
+        # CRT operand geometry and the constant Toeplitz digits T[pos][4 j + a] = byte (pos - a) of M / p_j
+        self.Kc = _round_up(4 * npr, 32)
+        P = 4 * ml + 3
+        self.NH = _round_up(-(-P // 2), 16)
+        mb = np.array([limbs(m, ml) for m in mj], dtype=np.uint32).view(np.uint8).reshape(npr, 4 * ml)
+        T = np.zeros((2 * self.NH, self.Kc), dtype=np.uint8)
+        for jj in range(npr):
+            for a in range(4):
+                T[a:a + 4 * ml, 4 * jj + a] = mb[jj]
+        tiles = [T[h * self.NH:(h + 1) * self.NH].reshape(self.NH // 8, 8, self.Kc // 16, 16).transpose(2, 0, 1, 3)
+                 for h in range(2)]
+        self.T = torch.from_numpy(np.ascontiguousarray(np.concatenate([t.reshape(-1) for t in tiles]))).to(device)
         self.c = RnsTables(self.p.data_ptr(), self.mu.data_ptr(), self.w.data_ptr(), self.conv.data_ptr(),
                            self.inv.data_ptr(), self.mj.data_ptr(), self.mfull.data_ptr(), self.rp.data_ptr(), npr, ml)
 
@@ -139,7 +157,7 @@ def _split(tb, m, plane, nb, R, K, sb, sr, sk, Kp, TR, stream):
     return out, mat, Rp
 
 
-def gemm_aligned_rns(Aal, Bal):
+def gemm_aligned_rns(Aal, Bal, crt="tensor"):
     """(row-aligned A (L, nb, M, K), (nb, M)) x (column-aligned B (L, nb, K, N), (nb, N)) -> MPF (nb, M, N),
     on the tensor cores; K <= 256"""
     am, ae = Aal
@@ -163,15 +181,25 @@ def gemm_aligned_rns(Aal, Bal):
     TN = min(256, _round_up(4 * NL, 16))
     X, x_mat, _ = _split(tb, xs["m"], xs["plane"], nb, xs["R"], K, xs["sb"], xs["sr"], xs["sk"], Kp, 128, stream)
     Y, y_mat, Rp_y = _split(tb, ys["m"], ys["plane"], nb, NL, K, ys["sb"], ys["sr"], ys["sk"], Kp, TN, stream)
-    res = torch.empty(tb.np * nb * M * N, dtype=torch.int32, device=dev)
-    args = RnsMmaArgs(X.data_ptr(), Y.data_ptr(), x_mat, y_mat, nb, xs["R"], NL, Kp, TN, (4 * Rp_y) // TN,
-                      M * N, out_i, out_l, res.data_ptr(), tb.err.data_ptr())
-    _check(_bind().b3d_rns_mma(ctypes.byref(args), ctypes.byref(tb.c), stream), "b3d_rns_mma")
-    cm = torch.empty((L, nb * M * N), dtype=torch.int32, device=dev)
+    n = nb * M * N
+    cm = torch.empty((L, n), dtype=torch.int32, device=dev)
     ce = torch.empty((nb, M, N), dtype=torch.int64, device=dev)
-    _check(_bind().b3d_rns_crt(L, res.data_ptr(), nb * M * N, ae.contiguous().data_ptr(), be.contiguous().data_ptr(),
-                               nb, M, N, ctypes.byref(tb.c), cm.data_ptr(), ce.data_ptr(), cm.stride(0), stream),
-           "b3d_rns_crt")
+    ae, be = ae.contiguous(), be.contiguous()
+    if crt == "tensor":                                     # y bytes -> CRT on the tensor cores
+        yb = torch.zeros(_round_up(max(n, 1), 128) * tb.Kc, dtype=torch.uint8, device=dev)
+        args = RnsMmaArgs(X.data_ptr(), Y.data_ptr(), x_mat, y_mat, nb, xs["R"], NL, Kp, TN, (4 * Rp_y) // TN,
+                          M * N, out_i, out_l, None, tb.err.data_ptr(), yb.data_ptr(), tb.Kc)
+        _check(_bind().b3d_rns_mma(ctypes.byref(args), ctypes.byref(tb.c), stream), "b3d_rns_mma")
+        cargs = RnsCrtArgs(yb.data_ptr(), tb.T.data_ptr(), tb.Kc, tb.NH, n, nb, M, N, ae.data_ptr(), be.data_ptr(),
+                           cm.data_ptr(), ce.data_ptr(), cm.stride(0), tb.err.data_ptr())
+        _check(_bind().b3d_rns_crt_mma(L, ctypes.byref(cargs), ctypes.byref(tb.c), stream), "b3d_rns_crt_mma")
+    else:                                                   # residues -> CRT on the CUDA cores
+        res = torch.empty(tb.np * n, dtype=torch.int32, device=dev)
+        args = RnsMmaArgs(X.data_ptr(), Y.data_ptr(), x_mat, y_mat, nb, xs["R"], NL, Kp, TN, (4 * Rp_y) // TN,
+                          M * N, out_i, out_l, res.data_ptr(), tb.err.data_ptr(), None, 0)
+        _check(_bind().b3d_rns_mma(ctypes.byref(args), ctypes.byref(tb.c), stream), "b3d_rns_mma")
+        _check(_bind().b3d_rns_crt(L, res.data_ptr(), n, ae.data_ptr(), be.data_ptr(), nb, M, N, ctypes.byref(tb.c),
+                                   cm.data_ptr(), ce.data_ptr(), cm.stride(0), stream), "b3d_rns_crt")
     return MPF(cm.reshape(L, nb, M, N), ce)
 
 

@@ -133,12 +133,31 @@ typedef struct b3d_rns_mma_args {
     int Kp, TN;              /* padded K (multiple of 32, <= 256), column tile (multiple of 16, <= 256) */
     int64_t tiles_l;         /* column tiles */
     int64_t out_b, out_i, out_l;   /* residue output strides (elements) */
-    uint32_t* out;           /* (np, nb, ...) residues */
+    uint32_t* out;           /* (np, nb, ...) residues, when yb is NULL */
     int* err;                /* device error flag, 0 = ok */
+    uint8_t* yb;             /* else: y_j = r_j (M/p_j)^-1 mod p_j bytes, row e, column 4 j, of the CRT operand */
+    int64_t crt_kp;          /* bytes per row of the CRT operand (multiple of 32) */
 } b3d_rns_mma_args;
 
 /* residues of X Y^T per prime with tcgen05.mma.kind::i8 (TMEM accumulators, bulk async copies) */
 int b3d_rns_mma(const b3d_rns_mma_args* args, const b3d_rns_tables* tb, void* stream);
+
+/* CRT on the tensor cores: A = y bytes (b3d_rns_mma with yb), T = constant Toeplitz digits of M / p_j
+ * (2 NH rows x Kc, built by blocksvibe_b200/rns.py), result rounded to an MPF like b3d_rns_crt */
+typedef struct b3d_rns_crt_args {
+    const uint8_t* A;
+    const uint8_t* T;
+    int Kc, NH;
+    int64_t n, nbatch, M, N;
+    const int64_t* ea;
+    const int64_t* eb;
+    int32_t* cm;
+    int64_t* ce;
+    int64_t cplane;
+    int* err;
+} b3d_rns_crt_args;
+
+int b3d_rns_crt_mma(int L, const b3d_rns_crt_args* args, const b3d_rns_tables* tb, void* stream);
 
 /* CRT reconstruction of (np, n) residues, element e = (b * M + i) * N + l, rounded with exponents
  * ea[b * M + i] + eb[b * N + l] -> normalised MPF C (n) */

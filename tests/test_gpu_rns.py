@@ -19,7 +19,8 @@ pytestmark = pytest.mark.gpu
     (42, 1, 66, 192, 96),      # 1280 bits, K near the limit
     (10, 1, 3, 256, 260),      # K = 256, N > one column tile
 ])
-def test_rns_gemm_bitwise_equals_schoolbook(cuda, L, nb, M, K, N):
+@pytest.mark.parametrize("crt", ["tensor", "cuda"])
+def test_rns_gemm_bitwise_equals_schoolbook(cuda, L, nb, M, K, N, crt):
     g = torch.Generator().manual_seed(L * 1000 + M + K + N)
     A = mpf.random_mpf((nb, M, K), L, spread=20, device=cuda, generator=g)
     B = mpf.random_mpf((nb, K, N), L, spread=20, device=cuda, generator=g)
@@ -28,7 +29,7 @@ def test_rns_gemm_bitwise_equals_schoolbook(cuda, L, nb, M, K, N):
     A.e[0, 0, 0] = mpf.EZ
     Aal, Bal = mpf.align_rows(A), mpf.align_cols(B)
     ref = mpf.gemm_aligned(Aal, Bal)
-    got = rns.gemm_aligned_rns(Aal, Bal)
+    got = rns.gemm_aligned_rns(Aal, Bal, crt=crt)
     torch.cuda.synchronize()
     rns.check_errors(cuda)
     assert torch.equal(ref.e, got.e)
@@ -45,5 +46,6 @@ def test_rns_gemm_cancellation(cuda):
     A.e[0, 1, :] = A.e[0, 0, :]
     Aal, Bal = mpf.align_rows(A), mpf.align_cols(B)
     ref = mpf.gemm_aligned(Aal, Bal)
-    got = rns.gemm_aligned_rns(Aal, Bal)
-    assert torch.equal(ref.m, got.m) and torch.equal(ref.e, got.e)
+    for crt in ("tensor", "cuda"):
+        got = rns.gemm_aligned_rns(Aal, Bal, crt=crt)
+        assert torch.equal(ref.m, got.m) and torch.equal(ref.e, got.e)
