@@ -21,6 +21,9 @@ SIGNATURES = {
     "b3d_cauchy_level": [_I, _P, _P, _Q, _P, _P, _Q, _P, _P, _P, _Q, _P],
     "b3d_pole_level": [_I, _P, _P, _Q, _P, _P, _Q, _P, _P, _Q, _P, _P, _P, _P, _Q, _Q, _I, _P, _P, _Q, _P, _P, _Q, _P],
     "b3d_moments_level": [_I, _P, _P, _Q, _P, _P, _Q, _P, _P, _P, _Q, _Q, _I, _P, _P, _Q, _P],
+    "b3d_cauchy_align": [_I, _P, _P, _Q, _P, _P, _P, _Q, _P],
+    "b3d_cauchy_digits": [_P, _P, _Q, _I, _Q, _Q, _I, _Q, _P, _P],
+    "b3d_cauchy_add_hinf": [_I, _P, _P, _Q, _P, _P, _Q, _P, _P, _P, _Q, _P],
     "b3d_pole_level_noalloc": [_I, _P, _P, _Q, _P, _P, _Q, _P, _P, _Q, _P, _P, _P, _P, _Q, _Q, _I, _P, _P, _Q, _P],
 }
 
@@ -32,6 +35,9 @@ class LevelTables(ctypes.Structure):
 
 
 SIGNATURES["b3d_cauchy_level"][7] = ctypes.POINTER(LevelTables)
+SIGNATURES["b3d_cauchy_align"][4] = ctypes.POINTER(LevelTables)
+SIGNATURES["b3d_cauchy_digits"][0] = ctypes.POINTER(LevelTables)
+SIGNATURES["b3d_cauchy_add_hinf"][7] = ctypes.POINTER(LevelTables)
 ctypes_byref = ctypes.byref
 
 

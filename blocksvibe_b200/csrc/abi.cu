@@ -133,6 +133,18 @@ int b3d_rns_split(int L, const int32_t* m, int64_t plane, int64_t nb, int64_t R,
                                               as_stream(stream)), "b3d_rns_split"));
 }
 
+int b3d_rns_split_mma(int L, const b3d_rns_split_args* a, const b3d_rns_tables* tb, void* stream) {
+    if (!a || !tb || tb->np != b3d::rns_primes(L) || a->nb < 0 || a->nb > 65535 || a->R < 0 || a->K < 0 ||
+        a->Rp < a->R || a->Kp < a->K || a->Kp % 32 || a->TR % 16 || a->TR <= 0 || (4 * a->Rp) % a->TR ||
+        a->mat_bytes < 4 * a->Rp * a->Kp || a->Ks % 32 || a->Ks < 4 * L || a->NS % 16 || a->NS <= 0 ||
+        a->NS > 256 || 2 * a->NS < 4 * tb->np || 128 * a->Ks + 2 * a->NS * a->Ks + tb->np * 512 > 200 * 1024)
+        return fail(B3D_E_ARG, "b3d_rns_split_mma: invalid sizes or tables");
+    b3d::RnsSplit c{a->m, a->plane, a->nb, a->R, a->K, a->sb, a->sr, a->sk, a->Rp, a->Kp, a->TR, a->mat_bytes,
+                    a->out, a->C, a->Ks, a->NS, a->err};
+    b3d::RnsTables t = tables_of(tb);
+    B3D_DISPATCH_RNS(L, cuda_status(RX::split_mma(c, t, as_stream(stream)), "b3d_rns_split_mma"));
+}
+
 int b3d_rns_mma(const b3d_rns_mma_args* a, const b3d_rns_tables* tb, void* stream) {
     if (!a || !tb || a->Kp <= 0 || a->Kp > 256 || a->Kp % 32 || a->TN < 16 || a->TN > 256 || a->TN % 16 ||
         a->nb <= 0 || a->nb > 65535 || tb->np <= 0 || tb->np > 65535 || a->NI < 0 || a->NL < 0 ||
@@ -165,6 +177,41 @@ int b3d_rns_crt(int L, const uint32_t* res, int64_t n, const int64_t* ea, const 
     b3d::RnsTables t = tables_of(tb);
     B3D_DISPATCH_RNS(L, cuda_status(RX::crt(res, n, ea, eb, nbatch, M, N, t, cm, ce, cplane, as_stream(stream)),
                                     "b3d_rns_crt"));
+}
+
+namespace {
+b3d::CauchyLevel level_of(const b3d_level_tables* lv) {
+    return b3d::CauchyLevel{lv->m, lv->nb, lv->Mr, lv->Kc, lv->N, lv->hlevels, lv->Jh, lv->gsrc, lv->gj,
+                            lv->rowd, lv->nrow, lv->cold, lv->ncol, lv->col};
+}
+bool level_ok(const b3d_level_tables* lv) {
+    return lv && lv->nb >= 0 && lv->Mr >= 0 && lv->Kc >= 0 && lv->N >= 0 && lv->m >= 0 && lv->m < lv->hlevels;
+}
+}  // namespace
+
+int b3d_cauchy_align(int L, const int32_t* rm, const int64_t* re, int64_t rplane, const b3d_level_tables* lv,
+                     int32_t* om, int64_t* oe, int64_t oplane, void* stream) {
+    if (!level_ok(lv)) return fail(B3D_E_ARG, "b3d_cauchy_align: invalid level description");
+    b3d::CauchyLevel c = level_of(lv);
+    B3D_DISPATCH_CAUCHY(L, cuda_status(CX::align(rm, re, rplane, c, om, oe, oplane, as_stream(stream)), "b3d_cauchy_align"));
+}
+
+int b3d_cauchy_digits(const b3d_level_tables* lv, const uint32_t* table, int64_t dmax, int np, int64_t Rp, int64_t Kp,
+                      int TR, int64_t mat_bytes, uint8_t* out, void* stream) {
+    if (!level_ok(lv) || dmax < 0 || np <= 0 || Rp < lv->Mr || Kp < lv->Kc || Kp % 32 || TR % 16 || TR <= 0 ||
+        (4 * Rp) % TR || mat_bytes < 4 * Rp * Kp)
+        return fail(B3D_E_ARG, "b3d_cauchy_digits: invalid sizes");
+    return cuda_status(b3d::cauchy_digits_launch(level_of(lv), table, dmax, np, Rp, Kp, TR, mat_bytes, out,
+                                                 as_stream(stream)), "b3d_cauchy_digits");
+}
+
+int b3d_cauchy_add_hinf(int L, const int32_t* am, const int64_t* ae, int64_t aplane, const int32_t* hm,
+                        const int64_t* he, int64_t hplane, const b3d_level_tables* lv, int32_t* om, int64_t* oe,
+                        int64_t oplane, void* stream) {
+    if (!level_ok(lv)) return fail(B3D_E_ARG, "b3d_cauchy_add_hinf: invalid level description");
+    b3d::CauchyLevel c = level_of(lv);
+    B3D_DISPATCH_CAUCHY(L, cuda_status(CX::add_hinf(am, ae, aplane, hm, he, hplane, c, om, oe, oplane, as_stream(stream)),
+                                       "b3d_cauchy_add_hinf"));
 }
 
 }  // extern "C"

@@ -4,9 +4,10 @@
 
 #include "kernels.cuh"
 #include "rns.cuh"
+#include "cauchy_rns.cuh"
 
 namespace b3d {
-#define B3D_DECL(L) extern template struct Launch<L>; extern template struct RnsLaunch<L>;
+#define B3D_DECL(L) extern template struct Launch<L>; extern template struct RnsLaunch<L>; extern template struct CauchyRnsLaunch<L>;
 B3D_FOR_EACH_L(B3D_DECL)
 #undef B3D_DECL
 
@@ -14,8 +15,10 @@ B3D_FOR_EACH_L(B3D_DECL)
 int fail(int code, const std::string& what);
 // 0 for cudaSuccess, else the error code with its message recorded
 int cuda_status(int code, const char* fn);
-// tensor-core residue product (rns_mma.cu)
+// tensor-core residue product and the Cauchy coefficient digits (rns_mma.cu)
 int rns_mma_launch(const RnsMma& a, const RnsTables& tb, cudaStream_t st);
+int cauchy_digits_launch(const CauchyLevel& lv, const uint32_t* table, int64_t dmax, int np, int64_t Rp, int64_t Kp,
+                         int TR, int64_t mat_bytes, uint8_t* out, cudaStream_t st);
 }  // namespace b3d
 
 #define B3D_DISPATCH_RNS(L, CALL)                                              \
@@ -27,6 +30,18 @@ int rns_mma_launch(const RnsMma& a, const RnsTables& tb, cudaStream_t st);
         case 30: { using RX = b3d::RnsLaunch<30>; return CALL; }               \
         case 34: { using RX = b3d::RnsLaunch<34>; return CALL; }               \
         case 42: { using RX = b3d::RnsLaunch<42>; return CALL; }               \
+        default: return b3d::fail(B3D_E_LIMBS, "no kernels compiled for L = " + std::to_string(L)); \
+    }
+
+#define B3D_DISPATCH_CAUCHY(L, CALL)                                           \
+    switch (L) {                                                               \
+        case 6: { using CX = b3d::CauchyRnsLaunch<6>; return CALL; }           \
+        case 10: { using CX = b3d::CauchyRnsLaunch<10>; return CALL; }         \
+        case 18: { using CX = b3d::CauchyRnsLaunch<18>; return CALL; }         \
+        case 26: { using CX = b3d::CauchyRnsLaunch<26>; return CALL; }         \
+        case 30: { using CX = b3d::CauchyRnsLaunch<30>; return CALL; }         \
+        case 34: { using CX = b3d::CauchyRnsLaunch<34>; return CALL; }         \
+        case 42: { using CX = b3d::CauchyRnsLaunch<42>; return CALL; }         \
         default: return b3d::fail(B3D_E_LIMBS, "no kernels compiled for L = " + std::to_string(L)); \
     }
 

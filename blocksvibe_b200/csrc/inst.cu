@@ -2,6 +2,7 @@
 #define B3D_DEFINE_LAUNCH
 #include "kernels.cuh"
 #include "rns.cuh"
+#include "cauchy_rns.cuh"
 
 #ifndef B3D_L
 #error "compile with -DB3D_L=<limbs>"
@@ -10,4 +11,5 @@
 namespace b3d {
 template struct Launch<B3D_L>;
 template struct RnsLaunch<B3D_L>;
+template struct CauchyRnsLaunch<B3D_L>;
 }

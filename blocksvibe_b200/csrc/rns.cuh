@@ -303,6 +303,160 @@ __global__ void __launch_bounds__(128, 1) k_rns_mma(RnsMma a, RnsTables tb) {
 #endif
 
 // ------------------------------------------------------------------------------------------------
+// 1'. digits on the tensor cores.  One CTA = a tile of 8 operand rows x 16 columns k (128 elements).  The
+// elements' magnitude bytes form A (128 rows x 4 L bytes, K-major in shared memory); the constant
+// C[(j, t)][d] = byte t of (2^(8 d) mod p_j) is B (two tiles of NS rows); S = A B^T holds
+// sum_d digit_d C[(j, t)][d] < 4 L 255^2, so r_j = sum_t S[4 j + t] 2^(8 t) mod p_j (sign applied after).
+// The residue digits are staged in shared memory and written as 16-byte chunks of the same K-major
+// digit matrices k_rns_split writes.
+struct RnsSplit {
+    const int32_t* m; int64_t plane, nb, R, K, sb, sr, sk;   // aligned operand
+    int64_t Rp, Kp; int TR; int64_t mat_bytes;               // output digit matrices
+    uint8_t* out;
+    const uint8_t* C;        // (2 NS x Ks) constant digit matrix, tiles of NS rows
+    int Ks, NS;              // K bytes of the magnitudes (multiple of 32) and half of the 4 np columns
+    int* err;
+};
+
+#ifdef B3D_DEFINE_LAUNCH
+template <int L>
+__global__ void __launch_bounds__(128, 1) k_rns_split_mma(RnsSplit a, RnsTables tb) {
+    extern __shared__ __align__(128) uint8_t smem[];
+    __shared__ __align__(8) uint64_t bar_load, bar_mma;
+    __shared__ uint32_t tmem_base_sh;
+    __shared__ int fail_sh;
+    __shared__ uint8_t neg_sh[128];
+    const int Ks = a.Ks, NS = a.NS, np = tb.np;
+    uint8_t* sA = smem;                                  // 128 x Ks magnitude bytes
+    uint8_t* sC = smem + 128 * Ks;                       // 2 NS x Ks constants
+    uint8_t* sD = sC + 2 * NS * Ks;                      // np x 4 x 8 x 16 staged digits
+    const int warp = threadIdx.x / 32, t = threadIdx.x;
+    const int64_t b = blockIdx.y;
+    const int64_t ktiles = a.Kp / 16;
+    const int64_t r0 = (blockIdx.x / ktiles) * 8, k0 = (blockIdx.x % ktiles) * 16;
+    const uint32_t ncols = 512;
+    if (t == 0) {
+        fail_sh = 0;
+        mbar_init(&bar_load, 1);
+        mbar_init(&bar_mma, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                     ::"r"(smem_u32(&tmem_base_sh)), "r"(ncols) : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = tmem_base_sh;
+    if (t == 0) {
+        const uint32_t cbytes = 2u * NS * Ks;
+        mbar_expect_tx(&bar_load, cbytes);
+        bulk_copy_g2s(sC, a.C, cbytes, &bar_load);
+    }
+    // magnitudes of the tile's elements -> A rows e = rr * 16 + kk (load order follows the unit stride)
+    {
+        const bool rows_fast = a.sr == 1;
+        const int rr = rows_fast ? (t % 8) : (t / 16), kk = rows_fast ? (t / 8) : (t % 16);
+        const int e = rr * 16 + kk;
+        const int64_t r = r0 + rr, k = k0 + kk;
+        u32 v[L];
+        bool neg = false;
+        if (r < a.R && k < a.K) neg = load_mag<L>(a.m, a.plane, b * a.sb + r * a.sr + k * a.sk, v);
+        else zero(v);
+        neg_sh[e] = neg;
+#pragma unroll
+        for (int c = 0; c < (4 * L + 15) / 16; c++) {
+            uint4 w;
+            w.x = 4 * c + 0 < L ? v[4 * c + 0] : 0u;
+            w.y = 4 * c + 1 < L ? v[4 * c + 1] : 0u;
+            w.z = 4 * c + 2 < L ? v[4 * c + 2] : 0u;
+            w.w = 4 * c + 3 < L ? v[4 * c + 3] : 0u;
+            *reinterpret_cast<uint4*>(sA + tiled_offset(e, 16 * c, 128, Ks)) = w;
+        }
+        for (int c = (4 * L + 15) / 16; c < Ks / 16; c++)
+            *reinterpret_cast<uint4*>(sA + tiled_offset(e, 16 * c, 128, Ks)) = make_uint4(0, 0, 0, 0);
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");    // generic-proxy writes -> tensor core
+    if (!mbar_wait(&bar_load, 0, kWaitLimit)) atomicExch(&fail_sh, 1);
+    __syncthreads();
+    bool run = fail_sh == 0;
+    if (run && t == 0) {
+        const uint32_t idesc = (2u << 4) | ((uint32_t)(NS >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+        const uint32_t aa = smem_u32(sA), ac = smem_u32(sC);
+        for (int h = 0; h < 2; h++) {
+            for (int kk = 0; kk < Ks / 32; kk++) {
+                uint64_t da = umma_desc(aa + kk * 2 * (128 * 16), 128 * 16, 128);
+                uint64_t db = umma_desc(ac + h * NS * Ks + kk * 2 * (NS * 16), NS * 16, 128);
+                uint32_t acc = kk > 0 ? 1u : 0u;
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\t"
+                    "setp.ne.b32 p, %4, 0;\n\t"
+                    "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}"
+                    ::"r"(tmem + (uint32_t)(h * NS)), "l"(da), "l"(db), "r"(idesc), "r"(acc) : "memory");
+            }
+        }
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                     ::"r"(smem_u32(&bar_mma)) : "memory");
+    }
+    if (run && !mbar_wait(&bar_mma, 0, kWaitLimit)) atomicExch(&fail_sh, 2);
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    __syncthreads();
+    run = run && fail_sh == 0;
+    if (run) {
+        // epilogue: element e = t; residues of 4 primes per 16-column chunk
+        const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16);
+        const bool neg = neg_sh[t];
+        const int rr = t / 16, kk = t % 16;
+        for (int j0 = 0; j0 < np; j0 += 4) {
+            uint32_t d[16];
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+                "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
+                : "=r"(d[0]), "=r"(d[1]), "=r"(d[2]), "=r"(d[3]), "=r"(d[4]), "=r"(d[5]), "=r"(d[6]), "=r"(d[7]),
+                  "=r"(d[8]), "=r"(d[9]), "=r"(d[10]), "=r"(d[11]), "=r"(d[12]), "=r"(d[13]), "=r"(d[14]), "=r"(d[15])
+                : "r"(taddr + (uint32_t)(4 * j0)));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                const int j = j0 + q;
+                if (j >= np) break;
+                uint64_t v = (uint64_t)d[4 * q] + ((uint64_t)d[4 * q + 1] << 8) + ((uint64_t)d[4 * q + 2] << 16) +
+                             ((uint64_t)d[4 * q + 3] << 24);
+                const uint32_t p = __ldg(tb.p + j);
+                uint32_t r = barrett(v, p, __ldg(tb.mu + j));
+                if (neg && r) r = p - r;
+#pragma unroll
+                for (int s = 0; s < 4; s++) sD[((j * 4 + s) * 8 + rr) * 16 + kk] = (uint8_t)(r >> (8 * s));
+            }
+        }
+    }
+    __syncthreads();
+    if (run) {
+        // 16-byte chunks: (prime j, digit s, row rr) -> row 4 (r0 + rr) + s, columns k0 .. k0 + 15
+        for (int c = t; c < np * 32; c += 128) {
+            const int rr = c % 8, s = (c / 8) % 4, j = c / 32;
+            const int64_t r = r0 + rr;
+            if (r >= a.Rp) continue;
+            uint4 w = *reinterpret_cast<const uint4*>(sD + (size_t)c * 16);
+            *reinterpret_cast<uint4*>(a.out + ((size_t)j * a.nb + b) * a.mat_bytes + tiled_offset(4 * r + s, k0, a.TR, a.Kp)) = w;
+        }
+    }
+    if (t == 0 && fail_sh) {
+        if (!mbar_wait(&bar_load, 0, kWaitLimit)) fail_sh = 3;
+        else if (fail_sh == 2 && !mbar_wait(&bar_mma, 0, kWaitLimit)) fail_sh = 4;
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncols) : "memory");
+    }
+    if (t == 0 && fail_sh) atomicExch(a.err, fail_sh);
+}
+#endif
+
+// ------------------------------------------------------------------------------------------------
 // 3'. CRT on the tensor cores.  A = the y bytes of 128 outputs (rows e, K = 4 np bytes, from k_rns_mma),
 // B = the constant matrix T[pos][4 j + a] = byte (pos - a) of M / p_j (two tiles of NH rows), so that
 // S[e][pos] = sum_{j,a} y_{j,a}(e) T[pos][4 j + a] and x' = sum_pos S[pos] 2^(8 pos) = sum_j y_j M / p_j
@@ -520,6 +674,7 @@ struct RnsLaunch {
     static int crt(const uint32_t* res, int64_t n, const int64_t* ea, const int64_t* eb, int64_t nbatch, int64_t M,
                    int64_t N, const RnsTables& tb, int32_t* cm, int64_t* ce, int64_t cplane, cudaStream_t st);
     static int crt_mma(const RnsCrt& a, const RnsTables& tb, cudaStream_t st);
+    static int split_mma(const RnsSplit& a, const RnsTables& tb, cudaStream_t st);
 };
 
 #ifdef B3D_DEFINE_LAUNCH
@@ -538,6 +693,21 @@ int RnsLaunch<L>::crt(const uint32_t* res, int64_t n, const int64_t* ea, const i
                       int64_t N, const RnsTables& tb, int32_t* cm, int64_t* ce, int64_t cplane, cudaStream_t st) {
     if (n == 0) return 0;
     k_rns_crt<L><<<(unsigned)((n + 127) / 128), 128, 0, st>>>(res, n, ea, eb, nbatch, M, N, tb, cm, ce, cplane);
+    return (int)cudaGetLastError();
+}
+
+template <int L>
+int RnsLaunch<L>::split_mma(const RnsSplit& a, const RnsTables& tb, cudaStream_t st) {
+    static bool configured = false;
+    const int smem = 128 * a.Ks + 2 * a.NS * a.Ks + tb.np * 512;
+    if (!configured) {
+        int rc = (int)cudaFuncSetAttribute(k_rns_split_mma<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        if (rc) return rc;
+        configured = true;
+    }
+    if (a.nb == 0 || a.Rp == 0) return 0;
+    dim3 grid((unsigned)((a.Kp / 16) * ((a.Rp + 7) / 8)), (unsigned)a.nb);
+    k_rns_split_mma<L><<<grid, 128, smem, st>>>(a, tb);
     return (int)cudaGetLastError();
 }
 

@@ -18,4 +18,12 @@ int rns_mma_launch(const RnsMma& a, const RnsTables& tb, cudaStream_t st) {
     return (int)cudaGetLastError();
 }
 
+int cauchy_digits_launch(const CauchyLevel& lv, const uint32_t* table, int64_t dmax, int np, int64_t Rp, int64_t Kp,
+                         int TR, int64_t mat_bytes, uint8_t* out, cudaStream_t st) {
+    const int64_t n = lv.nb * Rp * (Kp / 4);
+    if (n == 0) return 0;
+    k_cauchy_digits<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(lv, table, dmax, np, Rp, Kp, TR, mat_bytes, out);
+    return (int)cudaGetLastError();
+}
+
 }  // namespace b3d

@@ -257,7 +257,7 @@ def gemm_aligned(Aal, Bal):
 # GEMM backend: "auto" (tensor-core RNS GEMM for 8 <= K <= 256, the CUDA-core schoolbook GEMM otherwise),
 # "rns" or "schoolbook" (both give the same bits: exact dot products, one rounding)
 GEMM_BACKEND = "auto"
-RNS_MIN_K = 64
+RNS_MIN_K = 32
 
 
 def _use_rns(K):

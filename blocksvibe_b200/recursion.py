@@ -25,7 +25,10 @@ class Recursion:
     """Numbers of one Plan on the GPU.  M: dict key -> matrix of decimal strings (keys as plan.Mkeys),
     an MPF table (nM, Smax, Smax) in plan.Mkeys order, or None for random O(1) matrices (timing runs)."""
 
-    def __init__(self, plan, M, L, device="cuda", generator=None):
+    def __init__(self, plan, M, L, device="cuda", generator=None, cauchy="cuda", rns_min_k=32):
+        """cauchy: "cuda" (one-limb divisions on the CUDA cores, b3d_cauchy_level), "rns" (the level's Cauchy
+        GEMM on the tensor cores, residues + CRT), or "auto" (rns for levels with at least rns_min_k columns)"""
+        self.cauchy, self.rns_min_k = cauchy, rns_min_k
         if not _lib.lib().b3d_supported_limbs(L):
             raise _lib.B3DError(f"no kernels compiled for L = {L}")
         if plan.dmax >= 1 << 16:
@@ -71,6 +74,73 @@ class Recursion:
         live = [d for d in self.levels if d]
         self.max_rows = max((d["nb"] * d["Mr"] for d in live), default=0)
         self.max_tasks = max((d["T"] for d in live), default=0)
+        self._ctable = None
+
+    def _cauchy_table(self):
+        """residues of round(2^(NB-1) / d), |d| <= dmax, per prime: (2 dmax + 1, np) on the device"""
+        if self._ctable is None:
+            from . import rns
+            tb = rns.tables(self.L, self.device)
+            ps = [int(x) & 0xFFFFFFFF for x in tb.p.cpu().tolist()]
+            NB, dm = mpf.nbits(self.L), self.plan.dmax
+            rows = []
+            for d in range(-dm, dm + 1):
+                if d == 0:
+                    rows.append([0] * len(ps))
+                    continue
+                a = abs(d)
+                q = ((1 << (NB - 1)) + a // 2) // a          # round half up on the magnitude
+                v = -q if d < 0 else q
+                rows.append([v % p for p in ps])
+            self._ctable = torch.tensor(np.array(rows, dtype=np.uint32).view(np.int32), device=self.device)
+        return self._ctable
+
+    def _use_rns(self, lev):
+        if self.cauchy == "cuda" or lev["m"] == 0 or lev["Kc"] > 256:
+            return False
+        return self.cauchy == "rns" or lev["Kc"] >= self.rns_min_k
+
+    def _cauchy_rns(self, lev, tabs, res, h_inf, H, stream):
+        """the level's Cauchy step as RNS GEMMs on the tensor cores, then + h_inf: H (nb Mr, N)"""
+        import ctypes
+        from . import rns
+        L, dev = self.L, self.device
+        nb, Mr, Kc, N = lev["nb"], lev["Mr"], lev["Kc"], tabs.N
+        p = lambda t: t.data_ptr()
+        tb = rns.tables(L, dev)
+        Xm = torch.empty((L, nb * Kc * N), dtype=torch.int32, device=dev)
+        Xe = torch.empty((nb, N), dtype=torch.int64, device=dev)
+        _lib.call("b3d_cauchy_align", L, p(res.m), p(res.e), res.m.stride(0), _lib.ctypes_byref(tabs), p(Xm), p(Xe),
+                  Xm.stride(0), stream)
+        Kp = -(-Kc // 32) * 32
+        table = self._cauchy_table()
+        c_rows = Mr >= N                                           # C on the 128 TMEM lanes
+        TN = min(256, -(-4 * (N if c_rows else Mr) // 16) * 16)
+        TRc = 128 if c_rows else TN
+        Rp_c = -(-Mr // (TRc // 4)) * (TRc // 4)
+        c_mat = 4 * Rp_c * Kp
+        C = torch.empty(tb.np * nb * c_mat, dtype=torch.uint8, device=dev)
+        _lib.call("b3d_cauchy_digits", _lib.ctypes_byref(tabs), p(table), self.plan.dmax, tb.np, Rp_c, Kp, TRc, c_mat,
+                  p(C), stream)
+        X, x_mat, Rp_x = rns._split(tb, Xm, Xm.stride(0), nb, N, Kc, Kc * N, 1, N, Kp, TN if c_rows else 128, stream)
+        if c_rows:
+            A, a_mat, B8, b_mat, NI, NL, Rp_l, oi, ol = C, c_mat, X, x_mat, Mr, N, Rp_x, N, 1
+        else:
+            A, a_mat, B8, b_mat, NI, NL, Rp_l, oi, ol = X, x_mat, C, c_mat, N, Mr, Rp_c, 1, N
+        n = nb * Mr * N
+        # the CRT operand's padding columns meet zero rows of the constant matrix: no clearing needed
+        yb = torch.empty((-(-n // 128) * 128) * tb.Kc, dtype=torch.uint8, device=dev)
+        args = rns.RnsMmaArgs(p(A), p(B8), a_mat, b_mat, nb, NI, NL, Kp, TN, (4 * Rp_l) // TN, Mr * N, oi, ol,
+                              None, p(tb.err), p(yb), tb.Kc)
+        rns._check(rns._bind().b3d_rns_mma(ctypes.byref(args), ctypes.byref(tb.c), stream), "b3d_rns_mma")
+        Hm = torch.empty((L, n), dtype=torch.int32, device=dev)
+        He = torch.empty(n, dtype=torch.int64, device=dev)
+        ea = torch.full((nb, Mr), 2 - mpf.nbits(L), dtype=torch.int64, device=dev)
+        cargs = rns.RnsCrtArgs(p(yb), p(tb.T), tb.Kc, tb.NH, n, nb, Mr, N, p(ea), p(Xe), p(Hm), p(He), Hm.stride(0),
+                               p(tb.err))
+        rns._check(rns._bind().b3d_rns_crt_mma(L, ctypes.byref(cargs), ctypes.byref(tb.c), stream), "b3d_rns_crt_mma")
+        _lib.call("b3d_cauchy_add_hinf", L, p(Hm), p(He), Hm.stride(0), p(h_inf.m), p(h_inf.e), h_inf.m.stride(0),
+                  _lib.ctypes_byref(tabs), p(H.m), p(H.e), H.m.stride(0), stream)
 
     def footprint_bytes(self, B):
         """device bytes run() allocates for B right-hand sides (slots, Cauchy rows, pole scratch)"""
@@ -100,8 +170,11 @@ class Recursion:
             tabs = _lib.LevelTables(lev["m"], lev["nb"], lev["Mr"], lev["Kc"], N, hlevels, Jh,
                                     p(lev["gsrc"]), p(lev["gj"]), p(lev["rowd"]), p(lev["nrow"]),
                                     p(lev["cold"]), p(lev["ncol"]), p(lev["col"]))
-            _lib.call("b3d_cauchy_level", L, p(res.m), p(res.e), res.m.stride(0), p(h_inf.m), p(h_inf.e),
-                      h_inf.m.stride(0), _lib.ctypes_byref(tabs), p(H.m), p(H.e), H.m.stride(0), stream)
+            if self._use_rns(lev):
+                self._cauchy_rns(lev, tabs, res, h_inf, H, stream)
+            else:
+                _lib.call("b3d_cauchy_level", L, p(res.m), p(res.e), res.m.stride(0), p(h_inf.m), p(h_inf.e),
+                          h_inf.m.stride(0), _lib.ctypes_byref(tabs), p(H.m), p(H.e), H.m.stride(0), stream)
             _lib.call("b3d_pole_level", L, p(H.m), p(H.e), H.m.stride(0),
                       p(self.Ralign[0]), p(self.Ralign[1]), self.Ralign[0].stride(0),
                       p(self.QLalign[0]), p(self.QLalign[1]), self.QLalign[0].stride(0),

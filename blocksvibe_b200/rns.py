@@ -27,6 +27,12 @@ class RnsMmaArgs(ctypes.Structure):
                 ("out", _P), ("err", _P), ("yb", _P), ("crt_kp", _Q)]
 
 
+class RnsSplitArgs(ctypes.Structure):
+    _fields_ = [("m", _P), ("plane", _Q), ("nb", _Q), ("R", _Q), ("K", _Q), ("sb", _Q), ("sr", _Q), ("sk", _Q),
+                ("Rp", _Q), ("Kp", _Q), ("TR", _I), ("mat_bytes", _Q), ("out", _P), ("C", _P), ("Ks", _I), ("NS", _I),
+                ("err", _P)]
+
+
 class RnsCrtArgs(ctypes.Structure):
     _fields_ = [("A", _P), ("T", _P), ("Kc", _I), ("NH", _I), ("n", _Q), ("nbatch", _Q), ("M", _Q), ("N", _Q),
                 ("ea", _P), ("eb", _P), ("cm", _P), ("ce", _P), ("cplane", _Q), ("err", _P)]
@@ -41,7 +47,9 @@ def _bind():
     lib.b3d_rns_mma.argtypes = [ctypes.POINTER(RnsMmaArgs), ctypes.POINTER(RnsTables), _P]
     lib.b3d_rns_crt.argtypes = [_I, _P, _Q, _P, _P, _Q, _Q, _Q, ctypes.POINTER(RnsTables), _P, _P, _Q, _P]
     lib.b3d_rns_crt_mma.argtypes = [_I, ctypes.POINTER(RnsCrtArgs), ctypes.POINTER(RnsTables), _P]
-    for f in (lib.b3d_rns_layout, lib.b3d_rns_split, lib.b3d_rns_mma, lib.b3d_rns_crt, lib.b3d_rns_crt_mma):
+    lib.b3d_rns_split_mma.argtypes = [_I, ctypes.POINTER(RnsSplitArgs), ctypes.POINTER(RnsTables), _P]
+    for f in (lib.b3d_rns_layout, lib.b3d_rns_split, lib.b3d_rns_mma, lib.b3d_rns_crt, lib.b3d_rns_crt_mma,
+              lib.b3d_rns_split_mma):
         f.restype = _I
     lib._rns_bound = True
     return lib
@@ -128,6 +136,19 @@ class Tables:
         tiles = [T[h * self.NH:(h + 1) * self.NH].reshape(self.NH // 8, 8, self.Kc // 16, 16).transpose(2, 0, 1, 3)
                  for h in range(2)]
         self.T = torch.from_numpy(np.ascontiguousarray(np.concatenate([t.reshape(-1) for t in tiles]))).to(device)
+        # split constants C[(j, t)][d] = byte t of (2^(8 d) mod p_j), d < 4 L: the magnitude bytes times C give
+        # the residues' byte-weighted sums
+        self.Ks = _round_up(4 * L, 32)
+        self.NS = _round_up(-(-4 * npr // 2), 16)
+        C = np.zeros((2 * self.NS, self.Ks), dtype=np.uint8)
+        for jj, p in enumerate(ps):
+            for d in range(4 * L):
+                v = pow(2, 8 * d, p)
+                for t4 in range(4):
+                    C[4 * jj + t4, d] = (v >> (8 * t4)) & 0xFF
+        tiles = [C[h * self.NS:(h + 1) * self.NS].reshape(self.NS // 8, 8, self.Ks // 16, 16).transpose(2, 0, 1, 3)
+                 for h in range(2)]
+        self.C = torch.from_numpy(np.ascontiguousarray(np.concatenate([t.reshape(-1) for t in tiles]))).to(device)
         self.c = RnsTables(self.p.data_ptr(), self.mu.data_ptr(), self.w.data_ptr(), self.conv.data_ptr(),
                            self.inv.data_ptr(), self.mj.data_ptr(), self.mfull.data_ptr(), self.rp.data_ptr(), npr, ml)
 
@@ -146,14 +167,22 @@ def _round_up(x, m):
     return -(-x // m) * m
 
 
+SPLIT = "tensor"          # "tensor": residue digits on the tensor cores; "cuda": on the CUDA cores
+
+
 def _split(tb, m, plane, nb, R, K, sb, sr, sk, Kp, TR, stream):
     """digit matrices (np, nb, 4 Rp x Kp) of an aligned operand with R rows, tiles of TR digit rows"""
     rows_per_tile = TR // 4
     Rp = _round_up(max(R, 1), rows_per_tile)
     mat = 4 * Rp * Kp
     out = torch.empty(tb.np * nb * mat, dtype=torch.uint8, device=m.device)
-    _check(_bind().b3d_rns_split(tb.L, m.data_ptr(), plane, nb, R, K, sb, sr, sk, Rp, Kp, TR, ctypes.byref(tb.c),
-                                 out.data_ptr(), mat, stream), "b3d_rns_split")
+    if SPLIT == "tensor":
+        args = RnsSplitArgs(m.data_ptr(), plane, nb, R, K, sb, sr, sk, Rp, Kp, TR, mat, out.data_ptr(),
+                            tb.C.data_ptr(), tb.Ks, tb.NS, tb.err.data_ptr())
+        _check(_bind().b3d_rns_split_mma(tb.L, ctypes.byref(args), ctypes.byref(tb.c), stream), "b3d_rns_split_mma")
+    else:
+        _check(_bind().b3d_rns_split(tb.L, m.data_ptr(), plane, nb, R, K, sb, sr, sk, Rp, Kp, TR, ctypes.byref(tb.c),
+                                     out.data_ptr(), mat, stream), "b3d_rns_split")
     return out, mat, Rp
 
 
@@ -186,7 +215,8 @@ def gemm_aligned_rns(Aal, Bal, crt="tensor"):
     ce = torch.empty((nb, M, N), dtype=torch.int64, device=dev)
     ae, be = ae.contiguous(), be.contiguous()
     if crt == "tensor":                                     # y bytes -> CRT on the tensor cores
-        yb = torch.zeros(_round_up(max(n, 1), 128) * tb.Kc, dtype=torch.uint8, device=dev)
+        # padding columns of the y bytes meet zero rows of the constant matrix T, padding rows are never stored
+        yb = torch.empty(_round_up(max(n, 1), 128) * tb.Kc, dtype=torch.uint8, device=dev)
         args = RnsMmaArgs(X.data_ptr(), Y.data_ptr(), x_mat, y_mat, nb, xs["R"], NL, Kp, TN, (4 * Rp_y) // TN,
                           M * N, out_i, out_l, None, tb.err.data_ptr(), yb.data_ptr(), tb.Kc)
         _check(_bind().b3d_rns_mma(ctypes.byref(args), ctypes.byref(tb.c), stream), "b3d_rns_mma")

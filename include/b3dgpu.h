@@ -125,6 +125,21 @@ int b3d_rns_split(int L, const int32_t* m, int64_t plane, int64_t nb, int64_t R,
                   int64_t sk, int64_t Rp, int64_t Kp, int TR, const b3d_rns_tables* tb, uint8_t* out,
                   int64_t mat_bytes, void* stream);
 
+/* the same digit matrices computed on the tensor cores: magnitude bytes x the constant C (2 NS x Ks) */
+typedef struct b3d_rns_split_args {
+    const int32_t* m;
+    int64_t plane, nb, R, K, sb, sr, sk;
+    int64_t Rp, Kp;
+    int TR;
+    int64_t mat_bytes;
+    uint8_t* out;
+    const uint8_t* C;
+    int Ks, NS;
+    int* err;
+} b3d_rns_split_args;
+
+int b3d_rns_split_mma(int L, const b3d_rns_split_args* args, const b3d_rns_tables* tb, void* stream);
+
 typedef struct b3d_rns_mma_args {
     const uint8_t* X;        /* lane-side digit matrices (tiles of 128 digit rows) */
     const uint8_t* Y;        /* column-side digit matrices (tiles of TN digit rows) */
@@ -164,6 +179,25 @@ int b3d_rns_crt_mma(int L, const b3d_rns_crt_args* args, const b3d_rns_tables* t
 int b3d_rns_crt(int L, const uint32_t* res, int64_t n, const int64_t* ea, const int64_t* eb, int64_t nbatch,
                 int64_t M, int64_t N, const b3d_rns_tables* tb, int32_t* cm, int64_t* ce, int64_t cplane,
                 void* stream);
+
+/* ---- the Cauchy step as an RNS GEMM on the tensor cores (the reference's "rns" Cauchy variant,
+ * recursion_gpu.py:456-460: C = +-2/k gathered from a table, bgemm(C, X)); per group g:
+ * H_raw[g] = C[g] X[g] with C[g][r][i] = round(2^(NB-1) / (rowd[g][r] - cold[g][i])) (fixed exponent 1 - NB),
+ * X[g][i][n] = res[col[g][i]][n] aligned per column. */
+
+/* X (nb, Kc, N) aligned per column (g, n) and its column exponents (nb, N) */
+int b3d_cauchy_align(int L, const int32_t* rm, const int64_t* re, int64_t rplane, const b3d_level_tables* lv,
+                     int32_t* om, int64_t* oe, int64_t oplane, void* stream);
+
+/* digit matrices of C (as b3d_rns_split writes them) from table[(d + dmax) * np + j] = residues of
+ * round(2^(NB-1) / d) */
+int b3d_cauchy_digits(const b3d_level_tables* lv, const uint32_t* table, int64_t dmax, int np, int64_t Rp, int64_t Kp,
+                      int TR, int64_t mat_bytes, uint8_t* out, void* stream);
+
+/* H = H_raw + h_inf rows of the level (one rounding); padded rows written as zero */
+int b3d_cauchy_add_hinf(int L, const int32_t* am, const int64_t* ae, int64_t aplane, const int32_t* hm,
+                        const int64_t* he, int64_t hplane, const b3d_level_tables* lv, int32_t* om, int64_t* oe,
+                        int64_t oplane, void* stream);
 
 /* Size of the device scratch array of b3d_pole_level_noalloc (per GPU, held until the process exits). */
 #define B3D_NOALLOC_SCRATCH_BYTES ((size_t)16 << 20)

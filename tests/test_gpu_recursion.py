@@ -45,9 +45,9 @@ def random_case(tj12, tj43, tjmax, order, pp, L, nrhs, seed):
     return M, H
 
 
-def check(tj12, tj43, tjmax, order, pp, L, nrhs, M, H, device, reuse=False):
+def check(tj12, tj43, tjmax, order, pp, L, nrhs, M, H, device, reuse=False, cauchy="auto"):
     plan = PL.Plan(tj12, tj43, tjmax, order, pp, reuse=reuse)
-    rec = RC.Recursion(plan, M, L, device=device)
+    rec = RC.Recursion(plan, M, L, device=device, cauchy=cauchy)
     res = mpf.to_mp(rec.run(hinf_tensor(H, plan, order, nrhs, L, device)))
     mp.mp.prec = 32 * L + 64
     Mn = {k: [[mp.mpf(x) for x in row] for row in v] for k, v in M.items()}
@@ -72,11 +72,13 @@ def check(tj12, tj43, tjmax, order, pp, L, nrhs, M, H, device, reuse=False):
     return float(worst)
 
 
+@pytest.mark.parametrize("cauchy", ["cuda", "rns"])
 @pytest.mark.parametrize("ci", range(4))
-def test_recursion_golden_operators(cuda, ci):
+def test_recursion_golden_operators(cuda, ci, cauchy):
     c = golden("recursion.json")[ci]
     M, H = golden_operator(c)
-    check(c["tj12"], c["tj43"], c["tj_max"], c["order"], tuple(tuple(x) for x in c["pp"]), c["L"], c["rhs"], M, H, cuda)
+    check(c["tj12"], c["tj43"], c["tj_max"], c["order"], tuple(tuple(x) for x in c["pp"]), c["L"], c["rhs"], M, H, cuda,
+          cauchy=cauchy)
 
 
 @pytest.mark.parametrize("case", [
@@ -85,10 +87,11 @@ def test_recursion_golden_operators(cuda, ci):
     (3, 1, 5, 6, ((0, 1), (1, 1)), 18, 2, 13),
     (2, 2, 6, 8, ((0, 0), (1, 1)), 34, 1, 14),
 ])
-def test_recursion_random_operators(cuda, case):
+@pytest.mark.parametrize("cauchy", ["cuda", "rns"])
+def test_recursion_random_operators(cuda, case, cauchy):
     tj12, tj43, tjmax, order, pp, L, nrhs, seed = case
     M, H = random_case(*case)
-    check(tj12, tj43, tjmax, order, pp, L, nrhs, M, H, cuda)
+    check(tj12, tj43, tjmax, order, pp, L, nrhs, M, H, cuda, cauchy=cauchy)
 
 
 def test_slot_reuse_same_live_residues(cuda):

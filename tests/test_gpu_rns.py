@@ -19,8 +19,9 @@ pytestmark = pytest.mark.gpu
     (42, 1, 66, 192, 96),      # 1280 bits, K near the limit
     (10, 1, 3, 256, 260),      # K = 256, N > one column tile
 ])
-@pytest.mark.parametrize("crt", ["tensor", "cuda"])
-def test_rns_gemm_bitwise_equals_schoolbook(cuda, L, nb, M, K, N, crt):
+@pytest.mark.parametrize("crt,split", [("tensor", "tensor"), ("cuda", "cuda"), ("tensor", "cuda")])
+def test_rns_gemm_bitwise_equals_schoolbook(cuda, L, nb, M, K, N, crt, split):
+    rns.SPLIT = split
     g = torch.Generator().manual_seed(L * 1000 + M + K + N)
     A = mpf.random_mpf((nb, M, K), L, spread=20, device=cuda, generator=g)
     B = mpf.random_mpf((nb, K, N), L, spread=20, device=cuda, generator=g)
