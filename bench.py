@@ -39,6 +39,7 @@ def parse():
     ap.add_argument("--schedule", default="batched", choices=("batched", "plain"))
     ap.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of the CPU-baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--sample", type=int, default=12, help="set644: number of task groups timed")
     return ap.parse_args()
 
 
@@ -360,10 +361,73 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+def run_set(args):
+    """--workload set644: a sample of the seeded 644-task set (groups of tasks sharing an operator), each group
+    run as one batched pass (all its tasks and lambda orders) and task by task with one recursion per lambda
+    order (the plain per-task path); operators are built before timing, h_inf is resident on the device"""
+    import torch
+    from blocksvibe_b200 import dropin as DI
+    from blocksvibe_b200.workloads import make_device_tasks, task_set_644
+    world, rank, local = dist_setup()
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    groups = task_set_644()
+    step = max(1, len(groups) // max(1, args.sample))
+    picked = groups[::step][:args.sample]
+    ntask = sum(n for _, n in picked)
+    t0 = time.perf_counter()
+    prepared = []
+    for gi, (c, n) in enumerate(picked):
+        G, tasks = make_device_tasks(c, n, dev, seed=gi)
+        t = tasks[0]
+        op = DI.Operator(G, t.pp, t.parity, None, t.two_js_internal, list(t.coordinates), [t.delta_1_plus_2], dev)
+        prepared.append((op, tasks, t.lambda_orders(G.Lambda), t.delta_1_plus_2))
+    torch.cuda.synchronize()
+    setup_s = time.perf_counter() - t0
+
+    def batched():
+        for op, tasks, ns, d12 in prepared:
+            op.apply_outputs(op.run_batched(tasks, ns), d12)
+
+    def plain():
+        for op, tasks, ns, d12 in prepared:
+            for task in tasks:
+                op.apply_outputs(op.run_plain([task], ns), d12)
+
+    out = {}
+    for name, fn in (("batched", batched), ("plain", plain)):
+        for _ in range(max(1, args.warmup)):
+            fn()
+        torch.cuda.synchronize()
+        barrier(world)
+        s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s0.record()
+        for _ in range(args.steps):
+            fn()
+        s1.record()
+        torch.cuda.synchronize()
+        out[name] = max_over_ranks(s0.elapsed_time(s1) / args.steps, world, dev)
+    if rank == 0:
+        line = {"metric": "blocks_3d tasks/s", "value": world * ntask / (out["batched"] / 1e3), "unit": "tasks/s",
+                "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": out["batched"],
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "mpf int32 limbs",
+                "data": "synthetic (seeded 644-task set sample, random M and h_inf)",
+                "config": {"workload": "set644", "groups": len(picked), "tasks": ntask,
+                           "group_sizes": [n for _, n in picked]},
+                "plain": {"value": world * ntask / (out["plain"] / 1e3), "ms_per_step": out["plain"]},
+                "batched_over_plain": out["plain"] / out["batched"], "setup_s": setup_s}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "set644":
+        run_set(args)
     else:
         run_ours(args)
 

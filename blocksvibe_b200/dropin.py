@@ -109,7 +109,7 @@ class Operator:
         G = self.group
         nq, no = len(tasks), len(ns)
         h = self.hinf_batch(tasks, ns)                                        # rhs = q * no + idx
-        d = self.der
+        d = self.der.for_order(self.der.R)                 # own accumulators: concurrent batches may share self
         d.start(nq * no)
         self.rec.run(h, hook=d.accumulate)
         S2 = self.plan.Smax ** 2

@@ -58,15 +58,43 @@ def task_set_644(seed=644):
     out = []
     while sum(n for _, n in out) < 644:
         tj = rng.choice(ext)
-        half = tj[0] % 2
-        j12 = [x for x in range(abs(tj[0] - tj[1]), tj[0] + tj[1] + 1, 2) if x % 2 == half]
-        j43 = [x for x in range(abs(tj[3] - tj[2]), tj[3] + tj[2] + 1, 2) if x % 2 == half]
+        j12 = list(range(abs(tj[0] - tj[1]), tj[0] + tj[1] + 1, 2))     # doubled j12 allowed by the external pair
+        j43 = list(range(abs(tj[3] - tj[2]), tj[3] + tj[2] + 1, 2))
         Lam = rng.choice((7, 11, 15))
         spin_top = rng.randint(4, 30)
-        c = dict(two_js=tj, tj12=rng.choice(j12), tj43=rng.choice(j43), tjmax=2 * spin_top + half, Lam=Lam,
+        tj12, tj43 = rng.choice(j12), rng.choice(j43)
+        c = dict(two_js=tj, tj12=tj12, tj43=tj43, tjmax=2 * spin_top + tj12 % 2, Lam=Lam,
                  order=2 * Lam + 18, kept=Lam + 9, precision=rng.choice((768, 896, 1024)),
                  coords=(rng.choice(("xt", "xt_radial")),), d12=f"{rng.uniform(-1, 1):.30f}",
-                 pp=rng.choice(PP_SETS), sign=rng.choice((1, -1)))
+                 pp=rng.choice(PP_SETS) if tj12 and tj43 else PP_SETS[0], sign=rng.choice((1, -1)))
         n = min(rng.randint(1, 22), 644 - sum(k for _, k in out))
         out.append((c, n))
     return out
+
+
+def make_device_tasks(c, nq, device, seed=0):
+    """nq tasks of config c with random h_inf generated on the device (large task sets)"""
+    G = group_of(c)
+    L = DI.limbs(G.precision)
+    plan = Plan(G.two_j12, G.two_j43, G.two_j_max, G.order, c["pp"])
+    gen = torch.Generator(device=device).manual_seed(seed)
+    tasks = []
+    for q in range(nq):
+        t = DI.Task((q, 0, 0, 0), c["sign"], c["pp"], list(range(c["tj12"] % 2, c["tjmax"] + 1, 2)), c["coords"], c["d12"])
+        for n in t.lambda_orders(G.Lambda):
+            t.h_inf[n] = random_mpf_device((2, G.order + 1, plan.Jh, plan.Smax ** 2), L, device, gen)
+        tasks.append(t)
+    return G, tasks
+
+
+def random_mpf_device(shape, L, device, gen, spread=2):
+    """random normalised values drawn on the device (|x| in about [2^-spread, 2^spread])"""
+    from math import prod
+    n = prod(shape)
+    NB = mpf.nbits(L)
+    m = torch.randint(-2 ** 31, 2 ** 31 - 1, (L, n), dtype=torch.int32, device=device, generator=gen)
+    top = NB - 32 * (L - 1)
+    hi = (m[L - 1].to(torch.int64) & ((1 << (top - 1)) - 1)) | (1 << (top - 1))    # positive, exactly NB bits
+    m[L - 1] = hi.to(torch.int32)
+    e = torch.randint(-spread, spread + 1, (n,), device=device, generator=gen) - NB
+    return mpf.MPF(m.reshape((L,) + tuple(shape)), e.reshape(shape))
