@@ -196,6 +196,15 @@ int b3d_cauchy_align(int L, const int32_t* rm, const int64_t* re, int64_t rplane
     B3D_DISPATCH_CAUCHY(L, cuda_status(CX::align(rm, re, rplane, c, om, oe, oplane, as_stream(stream)), "b3d_cauchy_align"));
 }
 
+int b3d_cauchy_level2(int L, const int32_t* xm, const int64_t* xe, int64_t xplane, const int32_t* hm,
+                      const int64_t* he, int64_t hplane, const b3d_level_tables* lv, int32_t* om, int64_t* oe,
+                      int64_t oplane, void* stream) {
+    if (!level_ok(lv)) return fail(B3D_E_ARG, "b3d_cauchy_level2: invalid level description");
+    b3d::CauchyLevel c = level_of(lv);
+    B3D_DISPATCH(L, cuda_status(LX::cauchy2(xm, xe, xplane, hm, he, hplane, c, om, oe, oplane, as_stream(stream)),
+                                "b3d_cauchy_level2"));
+}
+
 int b3d_cauchy_digits(const b3d_level_tables* lv, const uint32_t* table, int64_t dmax, int np, int64_t Rp, int64_t Kp,
                       int TR, int64_t mat_bytes, uint8_t* out, void* stream) {
     if (!level_ok(lv) || dmax < 0 || np <= 0 || Rp < lv->Mr || Kp < lv->Kc || Kp % 32 || TR % 16 || TR <= 0 ||

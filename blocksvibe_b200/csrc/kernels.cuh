@@ -193,6 +193,108 @@ __global__ void k_cauchy(const int32_t* __restrict__ rm, const i64* __restrict__
     oe[t] = eo;
 }
 
+
+// ------------------------------------------------------------------------------------------------
+// Cauchy step, second form: X already aligned per column (g, n) (k_cauchy_align: (nb, Kc, N) mantissas and the
+// column exponents).  Each term floor(|x| 2^32 / |d|) is produced limb by limb from the top and added with its
+// sign into per-limb 64-bit accumulators (no carry chain per term: |acc[k]| < Kc 2^32); two terms are divided
+// at once (independent chains); the digit corrections are branch free.  One carry pass, one rounding, then the
+// h_inf term is added with one more rounding (as k_cauchy).
+struct Div16 {
+    u32 d, inv;
+};
+
+__device__ __forceinline__ u32 div16_step(u32 cur, const Div16& v, u32* rem) {
+    u32 q = umulhi32(cur, v.inv);                 // inv = floor((2^32 - 1) / d): q is at most 2 short
+    u32 r = cur - q * v.d;
+    bool c1 = r >= v.d;
+    q += c1; r -= c1 ? v.d : 0u;
+    bool c2 = r >= v.d;
+    q += c2; r -= c2 ? v.d : 0u;
+    *rem = r;
+    return q;
+}
+
+template <int L>
+__global__ void k_cauchy2(const int32_t* __restrict__ xm, const i64* __restrict__ xe, i64 xplane,
+                          const int32_t* __restrict__ hm, const i64* __restrict__ he, i64 hplane,
+                          CauchyLevel lv, int32_t* __restrict__ om, i64* __restrict__ oe, i64 oplane) {
+    i64 t = blockIdx.x * (i64)blockDim.x + threadIdx.x;
+    const i64 N = lv.N;
+    if (t >= lv.nb * lv.Mr * N) return;
+    const i64 n = t % N, r = (t / N) % lv.Mr, g = t / (N * lv.Mr);
+    if (r >= lv.nrow[g]) {
+        u32 z[L];
+        zero(z);
+        store_signed<L>(om, oplane, t, z, false);
+        oe[t] = EZ;
+        return;
+    }
+    const i64 hidx = ((lv.gsrc[g] * lv.hlevels + lv.m) * lv.Jh + lv.gj[g]) * N + n;
+    const i64 E = xe[g * N + n];
+    const i64 ncol = lv.ncol[g];
+    const i64* cold = lv.cold + g * lv.Kc;
+    const i64 D = lv.rowd[g * lv.Mr + r];
+    long long acc[L + 1];
+#pragma unroll
+    for (int k = 0; k <= L; k++) acc[k] = 0;
+    if (E != EZ) {
+        for (i64 i = 0; i < ncol; i += 2) {
+            u32 a0[L], a1[L];
+            const bool two = i + 1 < ncol;
+            i64 d0 = D - cold[i], d1 = two ? D - cold[i + 1] : 0;
+            bool n0 = load_mag<L>(xm, xplane, (g * lv.Kc + i) * N + n, a0);
+            bool n1 = false;
+            if (two) n1 = load_mag<L>(xm, xplane, (g * lv.Kc + i + 1) * N + n, a1);
+            else zero(a1);
+            if (d0 < 0) { n0 = !n0; d0 = -d0; }
+            if (d1 < 0) { n1 = !n1; d1 = -d1; }
+            const bool live0 = d0 != 0, live1 = d1 != 0;
+            Div16 v0{live0 ? (u32)d0 : 1u, live0 ? 0xFFFFFFFFu / (u32)d0 : 0xFFFFFFFFu};
+            Div16 v1{live1 ? (u32)d1 : 1u, live1 ? 0xFFFFFFFFu / (u32)d1 : 0xFFFFFFFFu};
+            const long long s0 = !live0 ? 0 : (n0 ? -1 : 1), s1 = !live1 ? 0 : (n1 ? -1 : 1);
+            u32 r0 = 0, r1 = 0;
+#pragma unroll
+            for (int k = L; k >= 0; k--) {               // quotient limb k of floor(|x| 2^32 / d)
+                const u32 l0 = k > 0 ? a0[k - 1] : 0u, l1 = k > 0 ? a1[k - 1] : 0u;
+                u32 qh0 = div16_step((r0 << 16) | (l0 >> 16), v0, &r0);
+                u32 qh1 = div16_step((r1 << 16) | (l1 >> 16), v1, &r1);
+                u32 ql0 = div16_step((r0 << 16) | (l0 & 0xFFFFu), v0, &r0);
+                u32 ql1 = div16_step((r1 << 16) | (l1 & 0xFFFFu), v1, &r1);
+                acc[k] += s0 * (long long)((qh0 << 16) | ql0) + s1 * (long long)((qh1 << 16) | ql1);
+            }
+        }
+    }
+    // carry pass into L + 3 two's complement limbs, value acc 2^(E - 31)
+    u32 w[L + 3];
+    long long c = 0;
+#pragma unroll
+    for (int k = 0; k <= L; k++) {
+        long long v = acc[k] + c;
+        w[k] = (u32)v;
+        c = v >> 32;
+    }
+#pragma unroll
+    for (int k = L + 1; k < L + 3; k++) {
+        w[k] = (u32)c;
+        c >>= 32;
+    }
+    const bool neg = (w[L + 2] >> 31) != 0;
+    if (neg) negate(w);
+    u32 s[L];
+    i64 es;
+    bool ns = false;
+    if (E != EZ && round_mag<L>(w, E - 31, s, &es)) ns = neg;
+    else { zero(s); es = EZ; }
+    u32 h[L], out[L];
+    const bool nh = load_mag<L>(hm, hplane, hidx, h);
+    bool no;
+    i64 eo;
+    add_norm<L>(s, ns, es, h, nh, he[hidx], out, &no, &eo);
+    store_signed<L>(om, oplane, t, out, no);
+    oe[t] = eo;
+}
+
 // ------------------------------------------------------------------------------------------------
 // Pole step, stage 1: Y[t, a, b0, k] = sum_b R[b0, b] H[t_hrow[t], a, b, k]  (R = Rtab[t_R[t]] aligned
 // per row; H aligned per column (a, k) over b here).  Y: (T, S, S, B) contiguous.
@@ -346,6 +448,8 @@ struct Launch {
                    i64 bplane, const i64* bidx, i64 n, int32_t* cm, i64* ce, i64 cplane, cudaStream_t st);
     static int cauchy(const int32_t* rm, const i64* re, i64 rplane, const int32_t* hm, const i64* he, i64 hplane,
                       const CauchyLevel& lv, int32_t* om, i64* oe, i64 oplane, cudaStream_t st);
+    static int cauchy2(const int32_t* xm, const i64* xe, i64 xplane, const int32_t* hm, const i64* he, i64 hplane,
+                       const CauchyLevel& lv, int32_t* om, i64* oe, i64 oplane, cudaStream_t st);
     static int pole(const int32_t* hm, const i64* he, i64 hplane, const int32_t* Rm, const i64* Re, i64 Rplane,
                     const int32_t* Qm, const i64* Qe, i64 Qplane, const i64* t_hrow, const i64* t_R, const i64* t_qL,
                     const i64* t_slot, i64 T, i64 B, int S, int32_t* ym, i64* ye, i64 yplane,
@@ -398,6 +502,15 @@ int Launch<L>::cauchy(const int32_t* rm, const i64* re, i64 rplane, const int32_
     i64 n = lv.nb * lv.Mr * lv.N;
     if (n == 0) return 0;
     k_cauchy<L><<<grid_for(n, kThreads), kThreads, 0, st>>>(rm, re, rplane, hm, he, hplane, lv, om, oe, oplane);
+    return (int)cudaGetLastError();
+}
+
+template <int L>
+int Launch<L>::cauchy2(const int32_t* xm, const i64* xe, i64 xplane, const int32_t* hm, const i64* he, i64 hplane,
+                       const CauchyLevel& lv, int32_t* om, i64* oe, i64 oplane, cudaStream_t st) {
+    i64 n = lv.nb * lv.Mr * lv.N;
+    if (n == 0) return 0;
+    k_cauchy2<L><<<grid_for(n, kThreads), kThreads, 0, st>>>(xm, xe, xplane, hm, he, hplane, lv, om, oe, oplane);
     return (int)cudaGetLastError();
 }
 

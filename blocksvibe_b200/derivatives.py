@@ -124,6 +124,9 @@ class Derivs:
         self.Dout = self.NPout + R + 1
         self._moment_levels()
         self._constants()
+        # index tensors of finish_iter, built once (no host-to-device copies while a CUDA graph is captured)
+        self._jidx = torch.tensor([(tj - tj12 % 2) // 2 for tj in self.tjs], device=self.device)
+        self._orders = {}
 
     # ------------------------------------------------------------ moment bookkeeping per level
     def _moment_levels(self):
@@ -234,20 +237,28 @@ class Derivs:
         self.cidx_te = torch.tensor([e - t if t <= e else R1 for t, e in te], device=dev)
         self.hidx_te = torch.tensor([e * R1 + (e - t) if t <= e else R1 * R1 for t, e in te], device=dev)
         self.cb_te = mpf.from_ints([comb(e, t) if t <= e else 0 for t, e in te], [0] * len(te), L, (len(te),), dev)
+        self._cb_rows = {}
 
     def for_order(self, R):
         """the same stages for a smaller R (a higher lambda order of the task), sharing this object's
-        constants as slices (reference ``derivatives.py:434-446``)"""
+        constants as slices (reference ``derivatives.py:434-446``).  The constants of each R are built once;
+        every call returns a fresh object (its accumulators are its own)."""
         if R > self.R:
             raise ValueError(f"R = {R} > {self.R}")
+        base = self._orders.get(R)
+        if base is None:
+            base = object.__new__(Derivs)
+            base.__dict__.update(self.__dict__)
+            base.R, base.Dout = R, self.NPout + R + 1
+            R1, K = R + 1, self.NP + R + 1
+            base.Anum = MPF(self.Anum.m[:, :, :base.Dout, :K], self.Anum.e[:, :base.Dout, :K]).contiguous()
+            base.Ttab = MPF(self.Ttab.m[:, :, :R1, :R1], self.Ttab.e[:, :R1, :R1]).contiguous()
+            base.Wh = MPF(self.Wh.m[:, :R1], self.Wh.e[:R1]).contiguous()
+            base._small_constants()
+            base._orders = {}
+            self._orders[R] = base
         d = object.__new__(Derivs)
-        d.__dict__.update(self.__dict__)
-        d.R, d.Dout = R, self.NPout + R + 1
-        R1, K = R + 1, self.NP + R + 1
-        d.Anum = MPF(self.Anum.m[:, :, :d.Dout, :K], self.Anum.e[:, :d.Dout, :K]).contiguous()
-        d.Ttab = MPF(self.Ttab.m[:, :, :R1, :R1], self.Ttab.e[:, :R1, :R1]).contiguous()
-        d.Wh = MPF(self.Wh.m[:, :R1], self.Wh.e[:R1]).contiguous()
-        d._small_constants()
+        d.__dict__.update(base.__dict__)
         return d
 
     def footprint_bytes(self, B):
@@ -284,7 +295,7 @@ class Derivs:
         R1, N, Rw = R + 1, self.N, max(R, 1)
         S2 = self.plan.Smax ** 2
         Nc = 2 * N
-        jidx = torch.tensor([(tj - self.plan.tj12 % 2) // 2 for tj in self.tjs], device=dev)
+        jidx = self._jidx
         H = MPF(h_inf.m[:, :, :order + 1][:, :, :, jidx], h_inf.e[:, :order + 1][:, :, jidx])   # (2, o+1, Jo, S2, B)
         H = H.permute(1, 2, 0, 3, 4).contiguous().reshape(order + 1, Jo * Nc)
         c = mpf.gemm(self.Wh, H).reshape(R1, Jo, Nc).permute(1, 0, 2)                          # (Jo, R+1, Nc)
@@ -308,8 +319,10 @@ class Derivs:
             cz = mpf.cat([c[j0:j1].permute(1, 0, 2).contiguous(), mpf.zeros((1, J, Nc), L, dev)], 0)  # (d | 0, jo, col)
             T2 = R1 * R1
             cte = cz.take(self.cidx_te).contiguous()                                              # (T2, J, Nc)
-            P = mpf.mul(cte.reshape(-1), self.cb_te, bidx=torch.arange(T2, device=dev).repeat_interleave(J * Nc),
-                        shape=(T2, J, Nc))
+            key = J * Nc
+            if key not in self._cb_rows:
+                self._cb_rows[key] = torch.arange(T2, device=dev).repeat_interleave(J * Nc)
+            P = mpf.mul(cte.reshape(-1), self.cb_te, bidx=self._cb_rows[key], shape=(T2, J, Nc))
             P = mpf.add(P, Hm.take(self.hidx_te).contiguous())                                    # ((t, e), jo, col)
             P = P.reshape(R1, R1, J, Nc).permute(2, 0, 1, 3).contiguous().reshape(J, R1, R1 * Nc)  # (jo, t, e col)
             Bn = mpf.cat([a.reshape(J, NP, R1 * Nc), P], 1)                                       # (jo, i | t, e col)

@@ -106,9 +106,12 @@ class Operator:
 
     def run_batched(self, tasks, ns):
         """one recursion pass over every (structure, lambda order); numerators per order from the shared moments"""
+        return self.run_batched_h(self.hinf_batch(tasks, ns), len(tasks), ns)
+
+    def run_batched_h(self, h, nq, ns):
+        """run_batched on h_inf already on the device: MPF (2, order + 1, Jh, S^2, nq * len(ns))"""
         G = self.group
-        nq, no = len(tasks), len(ns)
-        h = self.hinf_batch(tasks, ns)                                        # rhs = q * no + idx
+        no = len(ns)
         d = self.der.for_order(self.der.R)                 # own accumulators: concurrent batches may share self
         d.start(nq * no)
         self.rec.run(h, hook=d.accumulate)
@@ -143,6 +146,42 @@ class Operator:
             host[c] = buf
         torch.cuda.current_stream(self.device).synchronize()
         return host
+
+
+class GraphStep:
+    """The batched step of nq tasks (every lambda order: recursion, moments, numerators, write_output maps)
+    captured once as a CUDA graph and replayed per batch: no host work between the ~10^3 launches of a step.
+    h: the static device input (2, order + 1, Jh, S^2, nq * len(ns)); out: the static device results."""
+
+    def __init__(self, op, nq, ns, d12):
+        self.op, self.nq, self.ns, self.d12 = op, nq, list(ns), d12
+        G, pl, L, dev = op.group, op.plan, op.L, op.device
+        shape = (2, G.order + 1, pl.Jh, pl.Smax ** 2, nq * len(ns))
+        self.h = mpf.zeros(shape, L, dev)
+        self.stage = mpf.zeros((nq * len(ns),) + shape[:-1], L, dev)
+        op.apply_outputs(op.run_batched_h(self.h, nq, ns), d12)        # warm-up: builds every cached table
+        torch.cuda.synchronize(dev)
+        self.graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(self.graph):
+            self.out = op.apply_outputs(op.run_batched_h(self.h, nq, ns), d12)
+        torch.cuda.synchronize(dev)
+
+    def load(self, tasks):
+        """copy the tasks' h_inf (host or device MPFs, one per lambda order) into the static input"""
+        k = 0
+        for t in tasks:
+            for n in self.ns:
+                self.stage.m[:, k].copy_(t.h_inf[n].m, non_blocking=True)
+                self.stage.e[k].copy_(t.h_inf[n].e, non_blocking=True)
+                k += 1
+        self.h.m.copy_(self.stage.m.permute(0, 2, 3, 4, 5, 1))
+        self.h.e.copy_(self.stage.e.permute(1, 2, 3, 4, 0))
+
+    def run(self, tasks=None):
+        if tasks is not None:
+            self.load(tasks)
+        self.graph.replay()
+        return self.out
 
 
 def run_group(group, tasks, M, device="cuda", schedule="batched", max_rhs=None):

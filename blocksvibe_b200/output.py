@@ -179,6 +179,7 @@ class Output:
             else:
                 raise ValueError(f"coordinate {coordinate!r}: only xt and xt_radial")
         self.nL = (Lam - parity) // 2 + 1
+        self._idx = {}                     # cached index tensors (no host copies while a CUDA graph is captured)
         self.Wmp = W
         self.W = mpf.from_mp(list(W.reshape(-1)), L, W.shape, device)
 
@@ -189,7 +190,10 @@ class Output:
         nL = nL or self.nL
         nq = B // nL
         X = num.reshape(Jo, Dout, R1, 2, S2, nq, nL).permute(2, 6, 0, 3, 4, 5, 1).contiguous()   # (e, idx, ...)
-        uidx = torch.tensor([e * nL + i for i, e in self.inputs], device=num.device)
+        key = ("u", nL)
+        if key not in self._idx:
+            self._idx[key] = torch.tensor([e * nL + i for i, e in self.inputs], device=num.device)
+        uidx = self._idx[key]
         X = X.reshape(R1 * nL, -1).take(uidx)
         out = mpf.gemm(self.W, X).reshape(len(self.outputs), Jo, 2, S2, nq, Dout)
         return out.permute(1, 2, 3, 4, 0, 5).contiguous()
@@ -209,7 +213,10 @@ def apply_per_order(out, nums):
         X = x.permute(2, 0, 3, 4, 5, 1).contiguous()                                             # (e, jo, p, s, q, d)
         if D < Dmax:
             X = mpf.cat([X, mpf.zeros((R1, Jo, 2, S2, nq, Dmax - D), x.L, x.device)], 5)
-        rows.append(X.reshape(R1, -1).take(torch.tensor(need, device=x.device)))
+        key = ("need", idx)
+        if key not in out._idx:
+            out._idx[key] = torch.tensor(need, device=x.device)
+        rows.append(X.reshape(R1, -1).take(out._idx[key]))
     X = mpf.cat(rows, 0)
     Jo, _, _, _, S2, nq = nums[0].shape
     res = mpf.gemm(out.W, X).reshape(len(out.outputs), Jo, 2, S2, nq, Dmax)

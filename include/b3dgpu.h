@@ -189,6 +189,12 @@ int b3d_rns_crt(int L, const uint32_t* res, int64_t n, const int64_t* ea, const 
 int b3d_cauchy_align(int L, const int32_t* rm, const int64_t* re, int64_t rplane, const b3d_level_tables* lv,
                      int32_t* om, int64_t* oe, int64_t oplane, void* stream);
 
+/* the Cauchy step of b3d_cauchy_level from X already aligned (b3d_cauchy_align): per-limb 64-bit accumulation
+ * of the one-limb quotients, two terms per thread, one rounding, plus the h_inf term (the CUDA-core form) */
+int b3d_cauchy_level2(int L, const int32_t* xm, const int64_t* xe, int64_t xplane, const int32_t* hm,
+                      const int64_t* he, int64_t hplane, const b3d_level_tables* lv, int32_t* om, int64_t* oe,
+                      int64_t oplane, void* stream);
+
 /* digit matrices of C (as b3d_rns_split writes them) from table[(d + dmax) * np + j] = residues of
  * round(2^(NB-1) / d) */
 int b3d_cauchy_digits(const b3d_level_tables* lv, const uint32_t* table, int64_t dmax, int np, int64_t Rp, int64_t Kp,

@@ -105,3 +105,17 @@ def test_result_same_alone_and_in_mix(cuda):
     k = (tuple(tasks[1].q4), tasks[1].sign)
     for c in alone[k][2]:
         assert np.array_equal(alone[k][2][c][0], mix[k][2][c][0]) and np.array_equal(alone[k][2][c][1], mix[k][2][c][1])
+
+
+def test_cuda_graph_step_equals_launched_step(cuda):
+    """the captured step, replayed on two different batches, gives the launched step's bits"""
+    G, tasks, M, _, _ = make_group(nq=2, seed=31, coords=("xt", "xt_radial"))
+    t = tasks[0]
+    ns = t.lambda_orders(G.Lambda)
+    op = DI.Operator(G, t.pp, t.parity, M, t.two_js_internal, list(t.coordinates), [t.delta_1_plus_2], cuda)
+    g = DI.GraphStep(op, 1, ns, t.delta_1_plus_2)
+    for task in tasks:
+        ref = op.apply_outputs(op.run_batched([task], ns), t.delta_1_plus_2)
+        got = g.run([task])
+        for c in ref:
+            assert torch.equal(ref[c].m, got[c].m) and torch.equal(ref[c].e, got[c].e), c

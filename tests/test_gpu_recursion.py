@@ -110,3 +110,19 @@ def test_slot_reuse_same_live_residues(cuda):
         logical = int(torch.nonzero(torch.as_tensor(a.phys) == la)[0])
         lb = b.phys_slot(logical)
         assert torch.equal(ra.m[:, la], rb.m[:, lb]) and torch.equal(ra.e[la], rb.e[lb])
+
+
+@pytest.mark.parametrize("case", [
+    (4, 2, 6, 9, ((0, 1), (1, 0)), 10, 3, 61),
+    (8, 8, 6, 8, ((0, 0), (1, 1)), 34, 2, 62),
+])
+def test_cauchy_forms_bitwise_equal(cuda, case):
+    """the pre-aligned two-terms-per-thread Cauchy kernel gives the first kernel's bits"""
+    tj12, tj43, tjmax, order, pp, L, nrhs, seed = case
+    M, H = random_case(*case)
+    plan = PL.Plan(tj12, tj43, tjmax, order, pp, reuse=True)
+    outs = []
+    for form in ("cuda", "cuda2"):
+        rec = RC.Recursion(plan, M, L, device=cuda, cauchy=form)
+        outs.append(rec.run(hinf_tensor(H, plan, order, nrhs, L, cuda)))
+    assert torch.equal(outs[0].m, outs[1].m) and torch.equal(outs[0].e, outs[1].e)
