@@ -162,6 +162,25 @@ def peaks():
     return 6650.0, "fallback"
 
 
+def int8_peak_tops(device):
+    """dense INT8 tensor throughput of this GPU, measured with a plain library GEMM (torch._int_mm on 8192^3,
+    best of 5): the denominator of the RNS GEMM's tensor roofline (no INT8 figure is in MEASURED_PEAKS.json)"""
+    import torch
+    n = 8192
+    a = torch.randint(-128, 127, (n, n), dtype=torch.int8, device=device)
+    b = torch.randint(-128, 127, (n, n), dtype=torch.int8, device=device)
+    best = None
+    for _ in range(6):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        torch._int_mm(a, b)
+        e.record()
+        torch.cuda.synchronize()
+        t = s.elapsed_time(e) / 1e3
+        best = t if best is None else min(best, t)
+    return 2 * n ** 3 / best / 1e12
+
+
 def profile_traffic(kernel, workload):
     """dram bytes per launch of `kernel` from the committed ncu summary of this workload, if any"""
     path = os.path.join(ROOT, "profiles", f"{kernel}_{workload}.md")
@@ -346,6 +365,21 @@ def run_ours(args):
         roof = {"kernel": dominant, "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                 "frac": achieved / hbm, "peak_source": peak_kind, "traffic": traffic,
                 "algorithmic_bytes_per_launch": per_step_bytes / nl, "mean_launch_ms": statistics.mean(kernel_ms)}
+    # tensor roofline of the residue GEMM kernel (k_rns_mma): algorithmic int8 MACs / its event-timed launches
+    from blocksvibe_b200 import rns as RNS
+    RNS.MMA_TIMER, RNS.MMA_STATS["alg_macs"], RNS.MMA_STATS["macs"] = [], 0, 0
+    op.apply_outputs(run([dtask], ns), t.delta_1_plus_2)
+    torch.cuda.synchronize()
+    tensor_roof = None
+    if RNS.MMA_TIMER:
+        mma_s = sum(s.elapsed_time(e) for s, e in RNS.MMA_TIMER) / 1e3
+        peak8 = int8_peak_tops(dev)
+        ach = 2 * RNS.MMA_STATS["alg_macs"] / mma_s / 1e12
+        tensor_roof = {"kernel": "k_rns_mma (tcgen05.mma.kind::i8)", "bound": "tensor", "achieved": ach, "peak": peak8,
+                       "unit": "TOPS", "frac": ach / peak8, "peak_source": "measured here: torch._int_mm 8192^3",
+                       "issued_over_algorithmic": RNS.MMA_STATS["macs"] / RNS.MMA_STATS["alg_macs"],
+                       "launches_per_step": len(RNS.MMA_TIMER), "ms_per_step": mma_s * 1e3}
+    RNS.MMA_TIMER = None
     if rank != 0:
         if world > 1:
             import torch.distributed as dist
@@ -372,7 +406,7 @@ def run_ours(args):
             "other_schedule": {"schedule": "plain" if args.schedule == "batched" else "batched",
                                "value": world / (other_ms / 1e3), "ms_per_step": other_ms},
             "kernel_split_ms": {k: round(v, 3) for k, v in sorted(split.items(), key=lambda x: -x[1])},
-            "roofline": roof, "cpu_baseline": cpu, "clocks": clk}
+            "roofline": roof, "tensor_roofline": tensor_roof, "cpu_baseline": cpu, "clocks": clk}
     print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as dist

@@ -169,6 +169,11 @@ def _round_up(x, m):
 
 SPLIT = "tensor"          # "tensor": residue digits on the tensor cores; "cuda": on the CUDA cores
 
+# int8 multiply-accumulates issued to the tensor cores by the residue products since the last reset (the work
+# of k_rns_mma: 128 x TN x Kp per CTA), for the INT8 roofline
+MMA_STATS = {"macs": 0, "alg_macs": 0, "calls": 0}
+MMA_TIMER = None          # a list: (start, end) CUDA events are appended around every tensor-core product launch
+
 
 def _split(tb, m, plane, nb, R, K, sb, sr, sk, Kp, TR, stream):
     """digit matrices (np, nb, 4 Rp x Kp) of an aligned operand with R rows, tiles of TR digit rows"""
@@ -214,12 +219,21 @@ def gemm_aligned_rns(Aal, Bal, crt="tensor"):
     cm = torch.empty((L, n), dtype=torch.int32, device=dev)
     ce = torch.empty((nb, M, N), dtype=torch.int64, device=dev)
     ae, be = ae.contiguous(), be.contiguous()
+    MMA_STATS["macs"] += tb.np * nb * (x_mat // Kp) * TN * (4 * Rp_y // TN) * Kp
+    MMA_STATS["alg_macs"] += tb.np * nb * M * N * K * 16         # 4 x 4 byte products per residue product
+    MMA_STATS["calls"] += 1
     if crt == "tensor":                                     # y bytes -> CRT on the tensor cores
         # padding columns of the y bytes meet zero rows of the constant matrix T, padding rows are never stored
         yb = torch.empty(_round_up(max(n, 1), 128) * tb.Kc, dtype=torch.uint8, device=dev)
         args = RnsMmaArgs(X.data_ptr(), Y.data_ptr(), x_mat, y_mat, nb, xs["R"], NL, Kp, TN, (4 * Rp_y) // TN,
                           M * N, out_i, out_l, None, tb.err.data_ptr(), yb.data_ptr(), tb.Kc)
+        if MMA_TIMER is not None:
+            ev = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+            ev[0].record()
         _check(_bind().b3d_rns_mma(ctypes.byref(args), ctypes.byref(tb.c), stream), "b3d_rns_mma")
+        if MMA_TIMER is not None:
+            ev[1].record()
+            MMA_TIMER.append(ev)
         cargs = RnsCrtArgs(yb.data_ptr(), tb.T.data_ptr(), tb.Kc, tb.NH, n, nb, M, N, ae.data_ptr(), be.data_ptr(),
                            cm.data_ptr(), ce.data_ptr(), cm.stride(0), tb.err.data_ptr())
         _check(_bind().b3d_rns_crt_mma(L, ctypes.byref(cargs), ctypes.byref(tb.c), stream), "b3d_rns_crt_mma")
