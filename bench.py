@@ -209,6 +209,64 @@ def cpu_baseline(c, budget, cores):
                        f"MACs per right-hand side x {nrhs} lambda orders): recursion only, an upper bound on CPU tasks/s")}
 
 
+def json_measure(op, G, t, outs, dev, steps, cpu):
+    """blocks_3d's per-spin JSON files of one task from the step's device outputs (the writer after the
+    drop-in boundary, GPU-formatted): device time of its three kernels (CUDA events), end-to-end time with the
+    device-to-host copy of the text, and (cpu) the oracle's formatter timed on a sample of the same numbers"""
+    import torch
+    from blocksvibe_b200 import jsonout as JO
+    opts = JO.task_options(G, t)
+    outputs = {c: list(o.outputs) for (c, d), o in op.outs.items() if d == t.delta_1_plus_2}
+    x0 = next(iter(outs.values()))
+    w = JO.SpinWriter(opts, sorted(t.two_js_internal), t.pp, outputs, op.plan.Smax, 1, x0.shape[-1], dev)
+    t0 = time.perf_counter()
+    files = w.render(outs)                                 # builds the tables and caches the skeleton
+    first_s = time.perf_counter() - t0
+    text_bytes = sum(len(f) for f in files.values())
+    n = w.last_numbers
+    per = {}
+    e2e = []
+    for _ in range(steps):
+        ev = []
+        w.render_device(outs, 0, events=ev)
+        torch.cuda.synchronize()
+        for name, a, b in ev:
+            per.setdefault(name, []).append(a.elapsed_time(b))
+        s0 = time.perf_counter()
+        w.render(outs)
+        torch.cuda.synchronize()
+        e2e.append(time.perf_counter() - s0)
+    dev_ms = sum(statistics.mean(v) for v in per.values())
+    alg = n * (4 * x0.L + 8) + text_bytes                 # numbers read once, text written once
+    hbm, kind = peaks()
+    res = {"files": len(files), "numbers": n, "text_bytes": text_bytes, "digits": w.p,
+           "kernel_ms": {k: round(statistics.mean(v), 4) for k, v in per.items()}, "device_ms": dev_ms,
+           "e2e_ms": statistics.mean(e2e) * 1e3, "e2e_what": "device kernels + copy of the text to pinned host memory",
+           "first_render_s": first_s,
+           "roofline": {"kernels": "b3d_format_decimal + b3d_poly_sizes + b3d_emit_text", "bound": "hbm",
+                        "achieved": alg / (dev_ms / 1e3) / 1e9, "peak": hbm, "unit": "GB/s",
+                        "frac": alg / (dev_ms / 1e3) / 1e9 / hbm, "peak_source": kind,
+                        "algorithmic_bytes": alg}}
+    if cpu:
+        import numpy as np
+        from oracle import jsonfmt as OJ
+        m = x0.m.reshape(x0.L, -1)[:, :400].cpu().numpy().astype(np.int64) & 0xFFFFFFFF
+        e = x0.e.reshape(-1)[:400].cpu().numpy()
+        vals = []
+        for i in range(m.shape[1]):
+            v = int.from_bytes(m[:, i].astype("<u4").tobytes(), "little", signed=True)
+            vals.append((v, int(e[i]) if v else 0))
+        s0 = time.perf_counter()
+        for v, ex in vals:
+            OJ.fmt(v, ex, w.p)
+        per_num = (time.perf_counter() - s0) / len(vals)
+        res["cpu_baseline"] = {"value": per_num * n, "unit": "s per task (number formatting)", "cores": 1,
+                               "kind": "port", "sample": f"oracle jsonfmt.fmt on {len(vals)} of the task's {n} numbers, "
+                                                         "extrapolated (the reference's production writer uses MPFR "
+                                                         "through gmpy2, not installed here)"}
+    return res
+
+
 def run_reference(args):
     """--impl reference: the reference's CPU path (the oracle port of recursion_ref) on the host cores"""
     from blocksvibe_b200.workloads import CONFIGS
@@ -346,6 +404,10 @@ def run_ours(args):
     barrier(world)
     e2e_s = max_over_ranks(e2e_s, world, dev)
 
+    # blocks_3d's JSON files of the task (GPU formatter), after the boundary
+    jout = json_measure(op, G, t, op.apply_outputs(run([dtask], ns), t.delta_1_plus_2), dev, args.steps,
+                        rank == 0 and world == 1 and not args.no_cpu_baseline)
+
     # roofline of the dominant kernel: algorithmic bytes per launch / mean launch time
     L, N, S = op.L, op.plan.Smax ** 2 * (len(ns) if args.schedule == "batched" else 1), op.plan.Smax
     levs = [lv for lv in op.plan.levels if lv]
@@ -406,7 +468,7 @@ def run_ours(args):
             "other_schedule": {"schedule": "plain" if args.schedule == "batched" else "batched",
                                "value": world / (other_ms / 1e3), "ms_per_step": other_ms},
             "kernel_split_ms": {k: round(v, 3) for k, v in sorted(split.items(), key=lambda x: -x[1])},
-            "roofline": roof, "tensor_roofline": tensor_roof, "cpu_baseline": cpu, "clocks": clk}
+            "roofline": roof, "tensor_roofline": tensor_roof, "json_output": jout, "cpu_baseline": cpu, "clocks": clk}
     print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as dist

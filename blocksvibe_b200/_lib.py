@@ -26,6 +26,9 @@ SIGNATURES = {
     "b3d_cauchy_digits": [_P, _P, _Q, _I, _Q, _Q, _I, _Q, _P, _P],
     "b3d_cauchy_add_hinf": [_I, _P, _P, _Q, _P, _P, _Q, _P, _P, _P, _Q, _P],
     "b3d_pole_level_noalloc": [_I, _P, _P, _Q, _P, _P, _Q, _P, _P, _Q, _P, _P, _P, _P, _Q, _Q, _I, _P, _P, _Q, _P],
+    "b3d_format_decimal": [_I, _P, _P, _Q, _Q, _P, _P, _P, _P, _P],
+    "b3d_poly_sizes": [_I, _P, _P, _Q, _P, _Q, _I, _I, _P, _P, _P, _P],
+    "b3d_emit_text": [_P, _I, _P, _P, _P, _P, _P, _P, _Q, _P, _P],
 }
 
 
@@ -35,6 +38,13 @@ class LevelTables(ctypes.Structure):
                 ("gsrc", _P), ("gj", _P), ("rowd", _P), ("nrow", _P), ("cold", _P), ("ncol", _P), ("col", _P)]
 
 
+class DecimalTables(ctypes.Structure):
+    """struct b3d_decimal_tables"""
+    _fields_ = [("pow5", _P), ("pow5_limbs", _P), ("bounds", _P), ("kmax", _I), ("fw", _I), ("p", _I),
+                ("stride", _I)]
+
+
+SIGNATURES["b3d_format_decimal"][5] = ctypes.POINTER(DecimalTables)
 SIGNATURES["b3d_cauchy_level"][7] = ctypes.POINTER(LevelTables)
 SIGNATURES["b3d_cauchy_align"][4] = ctypes.POINTER(LevelTables)
 SIGNATURES["b3d_cauchy_digits"][0] = ctypes.POINTER(LevelTables)

@@ -51,7 +51,7 @@ def build(force=False, verbose=False):
     nvcc = _nvcc()
     jobs = [[nvcc, *ARCH, *FLAGS, f"-DB3D_L={L}", "-c", os.path.join(CSRC, "inst.cu"),
              "-o", os.path.join(BUILD, f"inst_L{L}.o")] for L in LIMBS]
-    for unit in ("abi", "noalloc", "rns_mma"):
+    for unit in ("abi", "noalloc", "rns_mma", "json"):
         jobs.append([nvcc, *ARCH, *FLAGS, "-c", os.path.join(CSRC, f"{unit}.cu"), "-o", os.path.join(BUILD, f"{unit}.o")])
     with ThreadPoolExecutor(max_workers=min(len(jobs), os.cpu_count() or 4)) as ex:
         for log in ex.map(_run, jobs):

@@ -3,6 +3,7 @@
 #include "kernels.cuh"
 #include "rns.cuh"
 #include "cauchy_rns.cuh"
+#include "decimal.cuh"
 
 #ifndef B3D_L
 #error "compile with -DB3D_L=<limbs>"
@@ -12,4 +13,5 @@ namespace b3d {
 template struct Launch<B3D_L>;
 template struct RnsLaunch<B3D_L>;
 template struct CauchyRnsLaunch<B3D_L>;
+template struct DecimalLaunch<B3D_L>;
 }

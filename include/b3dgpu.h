@@ -220,6 +220,41 @@ int b3d_pole_level_noalloc(int L, const int32_t* hm, const int64_t* he, int64_t 
                            const int64_t* t_hrow, const int64_t* t_R, const int64_t* t_qL, const int64_t* t_slot,
                            int64_t T, int64_t B, int S, int32_t* rm, int64_t* re, int64_t rplane, void* stream);
 
+/* ---- blocks_3d's JSON output (reference blocksvibe/b3djson.py, called from cli._write_one, cli.py:471-490) ---- */
+
+/* Tables of the decimal formatter, built once per (L, p) by the caller: pow5 = 5^k for k = 0 .. kmax as rows of
+ * fw limbs (pow5_limbs[k] = limbs in use), bounds = 10^(p-1) and 10^p as two rows of L - 1 limbs; p = digits;
+ * stride = bytes per output slot (multiple of 16, p + 12 .. 416).  kmax = 3 p covers |v| >= 10^(-2p-1). */
+typedef struct b3d_decimal_tables {
+    const uint32_t* pow5;
+    const int32_t* pow5_limbs;
+    const uint32_t* bounds;
+    int kmax, fw, p, stride;
+} b3d_decimal_tables;
+
+/* Number i (m, e limb planes) printed as blocks_3d's writer prints it (b3djson.fmt_gmpy + limbs_to_mpfr,
+ * b3djson.py:56-80: MPFR "%.{p}g" of the exact value, ties to even) into out[i * stride ...], its length in
+ * len[i].  err: two int64 set by the caller to {0, INT64_MAX}; numbers outside the supported decimal range
+ * (|v| < 10^(-2p-1), or far above 10^p) get len -1, add 1 to err[0] and lower err[1] to their index.
+ * out must be 16-byte aligned. */
+int b3d_format_decimal(int L, const int32_t* m, const int64_t* e, int64_t plane, int64_t n,
+                       const b3d_decimal_tables* tb, char* out, int32_t* len, int64_t* err, void* stream);
+
+/* Per polynomial t (coefficients poly_num[t] + d, d < D, of the same m / e arrays): the kept size of
+ * blocks_3d's truncation of negligible top coefficients (b3djson.py:160-166, eps = 2^-eps_shift; 0 when all
+ * coefficients are zero) in size[t], and the byte length of its text (quoted numbers joined by ",\n", or
+ * "0" in quotes) in text_len[t], -1 if a kept coefficient has length -1; len = the lengths from
+ * b3d_format_decimal. */
+int b3d_poly_sizes(int L, const int32_t* m, const int64_t* e, int64_t plane, const int64_t* poly_num, int64_t npoly,
+                   int D, int eps_shift, const int32_t* len, int32_t* size, int64_t* text_len, void* stream);
+
+/* Text assembly (b3djson.write_spin / derivs_text, b3djson.py:150-198): for each polynomial t, the skeleton
+ * bytes skel[skel_off[t] .. skel_off[t+1]) and then its text (size[t] < 0: none) are written to
+ * out[out_off[t] ...], out_off[t] = sum over t' < t of the skeleton plus text lengths. */
+int b3d_emit_text(const char* slots, int stride, const int32_t* len, const int64_t* poly_num, const int32_t* size,
+                  const int64_t* out_off, const char* skel, const int64_t* skel_off, int64_t npoly, char* out,
+                  void* stream);
+
 #ifdef __cplusplus
 }
 #endif
