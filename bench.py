@@ -411,7 +411,7 @@ def run_ours(args):
     # roofline of the dominant kernel: algorithmic bytes per launch / mean launch time
     L, N, S = op.L, op.plan.Smax ** 2 * (len(ns) if args.schedule == "batched" else 1), op.plan.Smax
     levs = [lv for lv in op.plan.levels if lv]
-    if dominant in ("b3d_cauchy_level", "b3d_cauchy_level2"):
+    if dominant in ("b3d_cauchy_level", "b3d_cauchy_level2", "b3d_cauchy_level3"):
         per_step_bytes = sum(RL.cauchy_level_bytes(lv, N, L) for lv in levs if lv["m"] > 0 or dominant == "b3d_cauchy_level") \
             * (1 if args.schedule == "batched" else len(ns))
     elif dominant == "b3d_pole_level":

@@ -23,6 +23,7 @@ SIGNATURES = {
     "b3d_moments_level": [_I, _P, _P, _Q, _P, _P, _Q, _P, _P, _P, _Q, _Q, _I, _P, _P, _Q, _P],
     "b3d_cauchy_align": [_I, _P, _P, _Q, _P, _P, _P, _Q, _P],
     "b3d_cauchy_level2": [_I, _P, _P, _Q, _P, _P, _Q, _P, _P, _P, _Q, _P],
+    "b3d_cauchy_level3": [_I, _P, _P, _Q, _P, _P, _Q, _P, _Q, _P, _P, _Q, _P],
     "b3d_cauchy_digits": [_P, _P, _Q, _I, _Q, _Q, _I, _Q, _P, _P],
     "b3d_cauchy_add_hinf": [_I, _P, _P, _Q, _P, _P, _Q, _P, _P, _P, _Q, _P],
     "b3d_pole_level_noalloc": [_I, _P, _P, _Q, _P, _P, _Q, _P, _P, _Q, _P, _P, _P, _P, _Q, _Q, _I, _P, _P, _Q, _P],
@@ -49,6 +50,7 @@ SIGNATURES["b3d_cauchy_level"][7] = ctypes.POINTER(LevelTables)
 SIGNATURES["b3d_cauchy_align"][4] = ctypes.POINTER(LevelTables)
 SIGNATURES["b3d_cauchy_digits"][0] = ctypes.POINTER(LevelTables)
 SIGNATURES["b3d_cauchy_level2"][7] = ctypes.POINTER(LevelTables)
+SIGNATURES["b3d_cauchy_level3"][7] = ctypes.POINTER(LevelTables)
 SIGNATURES["b3d_cauchy_add_hinf"][7] = ctypes.POINTER(LevelTables)
 ctypes_byref = ctypes.byref
 

@@ -205,6 +205,16 @@ int b3d_cauchy_level2(int L, const int32_t* xm, const int64_t* xe, int64_t xplan
                                 "b3d_cauchy_level2"));
 }
 
+int b3d_cauchy_level3(int L, const int32_t* xm, const int64_t* xe, int64_t xplane, const int32_t* hm,
+                      const int64_t* he, int64_t hplane, const b3d_level_tables* lv, int64_t dmax, int32_t* om,
+                      int64_t* oe, int64_t oplane, void* stream) {
+    if (!level_ok(lv)) return fail(B3D_E_ARG, "b3d_cauchy_level3: invalid level description");
+    if (dmax < 1 || dmax >= (1 << 16)) return fail(B3D_E_ARG, "b3d_cauchy_level3: dmax must be in [1, 65535]");
+    b3d::CauchyLevel c = level_of(lv);
+    B3D_DISPATCH(L, cuda_status(LX::cauchy3(xm, xe, xplane, hm, he, hplane, c, dmax, om, oe, oplane, as_stream(stream)),
+                                "b3d_cauchy_level3"));
+}
+
 int b3d_cauchy_digits(const b3d_level_tables* lv, const uint32_t* table, int64_t dmax, int np, int64_t Rp, int64_t Kp,
                       int TR, int64_t mat_bytes, uint8_t* out, void* stream) {
     if (!level_ok(lv) || dmax < 0 || np <= 0 || Rp < lv->Mr || Kp < lv->Kc || Kp % 32 || TR % 16 || TR <= 0 ||

@@ -295,6 +295,129 @@ __global__ void k_cauchy2(const int32_t* __restrict__ xm, const i64* __restrict_
     oe[t] = eo;
 }
 
+// The Cauchy step with wide quotient digits: the same exact quotients floor(|x| 2^32 / d) as k_cauchy2, but
+// the dividend (32 (L + 1) bits) is consumed in W-bit digits from the top, W = 24 when every divisor of the
+// level is below 2^8 and 22 below 2^10 (16 otherwise): r < d < 2^(32 - W) keeps (r << W) | digit in 32 bits,
+// so one multiply-high step per digit covers W bits instead of 16.  Quotient digits are summed per digit
+// position in signed 32-bit registers (|sum| <= ncol (2^W - 1) < 2^31: ncol < 128 for W = 24, < 512 for
+// W = 22, checked by the launcher), then carried into limbs: the result is bit-identical to k_cauchy2.
+template <int L>
+__device__ __forceinline__ u32 dividend_bits(const u32 (&a)[L], int lo, int width) {
+    const int li = lo >> 5, bo = lo & 31;                   // dividend limb k = (k == 0 ? 0 : a[k - 1])
+    const u32 v0 = li == 0 ? 0u : a[li - 1];
+    const u32 v1 = (li + 1 <= L) ? a[li] : 0u;
+    const u32 v = bo ? ((v0 >> bo) | (v1 << (32 - bo))) : v0;
+    return width >= 32 ? v : (v & ((1u << width) - 1u));
+}
+
+template <int L, int W>
+__global__ void k_cauchy3(const int32_t* __restrict__ xm, const i64* __restrict__ xe, i64 xplane,
+                          const int32_t* __restrict__ hm, const i64* __restrict__ he, i64 hplane,
+                          CauchyLevel lv, int32_t* __restrict__ om, i64* __restrict__ oe, i64 oplane) {
+    constexpr int TB = 32 * (L + 1), ND = (TB + W - 1) / W;
+    i64 t = blockIdx.x * (i64)blockDim.x + threadIdx.x;
+    const i64 N = lv.N;
+    if (t >= lv.nb * lv.Mr * N) return;
+    const i64 n = t % N, r = (t / N) % lv.Mr, g = t / (N * lv.Mr);
+    if (r >= lv.nrow[g]) {
+        u32 z[L];
+        zero(z);
+        store_signed<L>(om, oplane, t, z, false);
+        oe[t] = EZ;
+        return;
+    }
+    const i64 hidx = ((lv.gsrc[g] * lv.hlevels + lv.m) * lv.Jh + lv.gj[g]) * N + n;
+    const i64 E = xe[g * N + n];
+    const i64 ncol = lv.ncol[g];
+    const i64* cold = lv.cold + g * lv.Kc;
+    const i64 D = lv.rowd[g * lv.Mr + r];
+    int acc[ND];
+#pragma unroll
+    for (int j = 0; j < ND; j++) acc[j] = 0;
+    if (E != EZ) {
+        for (i64 i = 0; i < ncol; i += 2) {
+            u32 a0[L], a1[L];
+            const bool two = i + 1 < ncol;
+            i64 d0 = D - cold[i], d1 = two ? D - cold[i + 1] : 0;
+            bool n0 = load_mag<L>(xm, xplane, (g * lv.Kc + i) * N + n, a0);
+            bool n1 = false;
+            if (two) n1 = load_mag<L>(xm, xplane, (g * lv.Kc + i + 1) * N + n, a1);
+            else zero(a1);
+            if (d0 < 0) { n0 = !n0; d0 = -d0; }
+            if (d1 < 0) { n1 = !n1; d1 = -d1; }
+            const bool live0 = d0 != 0, live1 = d1 != 0;
+            const u32 v0 = live0 ? (u32)d0 : 1u, v1 = live1 ? (u32)d1 : 1u;
+            const u32 i0 = 0xFFFFFFFFu / v0, i1 = 0xFFFFFFFFu / v1;
+            const int s0 = !live0 ? 0 : (n0 ? -1 : 1), s1 = !live1 ? 0 : (n1 ? -1 : 1);
+            u32 r0 = 0, r1 = 0;
+#pragma unroll
+            for (int j = 0; j < ND; j++) {                  // digit j from the top: dividend bits [lo, lo + width)
+                const int lo = W * (ND - 1 - j);
+                const int width = j == 0 ? TB - W * (ND - 1) : W;
+                const u32 c0 = (r0 << width) | dividend_bits(a0, lo, width);
+                const u32 c1 = (r1 << width) | dividend_bits(a1, lo, width);
+                u32 q0 = umulhi32(c0, i0), q1 = umulhi32(c1, i1);   // at most 2 short
+                r0 = c0 - q0 * v0;
+                r1 = c1 - q1 * v1;
+                const bool x0 = r0 >= v0, x1 = r1 >= v1;
+                q0 += x0; r0 -= x0 ? v0 : 0u;
+                q1 += x1; r1 -= x1 ? v1 : 0u;
+                const bool y0 = r0 >= v0, y1 = r1 >= v1;
+                q0 += y0; r0 -= y0 ? v0 : 0u;
+                q1 += y1; r1 -= y1 ? v1 : 0u;
+                acc[j] += s0 * (int)q0 + s1 * (int)q1;
+            }
+        }
+    }
+    // digit sums -> signed limb sums (value sum_j acc[j] 2^(W (ND - 1 - j))), then the k_cauchy2 carry pass
+    long long accl[L + 2];
+#pragma unroll
+    for (int k = 0; k < L + 2; k++) accl[k] = 0;
+    {
+        long long carry = 0;
+#pragma unroll
+        for (int j = ND - 1; j >= 0; j--) {
+            const int lo = W * (ND - 1 - j), k0 = lo >> 5, b0 = lo & 31;
+            const long long v = (long long)acc[j] + carry;
+            long long part;
+            if (j > 0) {                                    // keep W bits here, carry the rest up
+                part = v & ((1ll << W) - 1);
+                carry = v >> W;
+            } else {
+                part = v;                                   // top digit: signed, small
+            }
+            // part 2^b0 = (part mod 2^(32 - b0)) 2^b0 + floor(part / 2^(32 - b0)) 2^32, exact for any part
+            const long long lo32 = b0 ? ((part & ((1ll << (32 - b0)) - 1)) << b0) : (part & 0xFFFFFFFFll);
+            const long long hi = b0 ? (part >> (32 - b0)) : (part >> 32);
+            accl[k0] += lo32;                               // k0 <= L: the dividend has L + 1 limbs
+            accl[k0 + 1] += hi;
+        }
+    }
+    u32 w[L + 3];
+    long long c = 0;
+#pragma unroll
+    for (int k = 0; k < L + 2; k++) {
+        long long v = accl[k] + c;
+        w[k] = (u32)v;
+        c = v >> 32;
+    }
+    w[L + 2] = (u32)c;
+    const bool neg = (w[L + 2] >> 31) != 0;
+    if (neg) negate(w);
+    u32 s[L];
+    i64 es;
+    bool ns = false;
+    if (E != EZ && round_mag<L>(w, E - 31, s, &es)) ns = neg;
+    else { zero(s); es = EZ; }
+    u32 h[L], out[L];
+    const bool nh = load_mag<L>(hm, hplane, hidx, h);
+    bool no;
+    i64 eo;
+    add_norm<L>(s, ns, es, h, nh, he[hidx], out, &no, &eo);
+    store_signed<L>(om, oplane, t, out, no);
+    oe[t] = eo;
+}
+
 // ------------------------------------------------------------------------------------------------
 // Pole step, stage 1: Y[t, a, b0, k] = sum_b R[b0, b] H[t_hrow[t], a, b, k]  (R = Rtab[t_R[t]] aligned
 // per row; H aligned per column (a, k) over b here).  Y: (T, S, S, B) contiguous.
@@ -450,6 +573,8 @@ struct Launch {
                       const CauchyLevel& lv, int32_t* om, i64* oe, i64 oplane, cudaStream_t st);
     static int cauchy2(const int32_t* xm, const i64* xe, i64 xplane, const int32_t* hm, const i64* he, i64 hplane,
                        const CauchyLevel& lv, int32_t* om, i64* oe, i64 oplane, cudaStream_t st);
+    static int cauchy3(const int32_t* xm, const i64* xe, i64 xplane, const int32_t* hm, const i64* he, i64 hplane,
+                       const CauchyLevel& lv, i64 dmax, int32_t* om, i64* oe, i64 oplane, cudaStream_t st);
     static int pole(const int32_t* hm, const i64* he, i64 hplane, const int32_t* Rm, const i64* Re, i64 Rplane,
                     const int32_t* Qm, const i64* Qe, i64 Qplane, const i64* t_hrow, const i64* t_R, const i64* t_qL,
                     const i64* t_slot, i64 T, i64 B, int S, int32_t* ym, i64* ye, i64 yplane,
@@ -511,6 +636,20 @@ int Launch<L>::cauchy2(const int32_t* xm, const i64* xe, i64 xplane, const int32
     i64 n = lv.nb * lv.Mr * lv.N;
     if (n == 0) return 0;
     k_cauchy2<L><<<grid_for(n, kThreads), kThreads, 0, st>>>(xm, xe, xplane, hm, he, hplane, lv, om, oe, oplane);
+    return (int)cudaGetLastError();
+}
+
+template <int L>
+int Launch<L>::cauchy3(const int32_t* xm, const i64* xe, i64 xplane, const int32_t* hm, const i64* he, i64 hplane,
+                       const CauchyLevel& lv, i64 dmax, int32_t* om, i64* oe, i64 oplane, cudaStream_t st) {
+    i64 n = lv.nb * lv.Mr * lv.N;
+    if (n == 0) return 0;
+    if (dmax < (1 << 8) && lv.Kc < 128)
+        k_cauchy3<L, 24><<<grid_for(n, kThreads), kThreads, 0, st>>>(xm, xe, xplane, hm, he, hplane, lv, om, oe, oplane);
+    else if (dmax < (1 << 10) && lv.Kc < 512)
+        k_cauchy3<L, 22><<<grid_for(n, kThreads), kThreads, 0, st>>>(xm, xe, xplane, hm, he, hplane, lv, om, oe, oplane);
+    else
+        k_cauchy2<L><<<grid_for(n, kThreads), kThreads, 0, st>>>(xm, xe, xplane, hm, he, hplane, lv, om, oe, oplane);
     return (int)cudaGetLastError();
 }
 

@@ -195,6 +195,13 @@ int b3d_cauchy_level2(int L, const int32_t* xm, const int64_t* xe, int64_t xplan
                       const int64_t* he, int64_t hplane, const b3d_level_tables* lv, int32_t* om, int64_t* oe,
                       int64_t oplane, void* stream);
 
+/* b3d_cauchy_level2 with wide quotient digits: the caller guarantees that every divisor |rowd - cold| of the
+ * level is at most dmax (the plan's maximum, < 2^16); with dmax < 2^8 (2^10) each multiply-high step of the
+ * one-limb division yields 24 (22) quotient bits instead of 16.  Results bit-identical to b3d_cauchy_level2. */
+int b3d_cauchy_level3(int L, const int32_t* xm, const int64_t* xe, int64_t xplane, const int32_t* hm,
+                      const int64_t* he, int64_t hplane, const b3d_level_tables* lv, int64_t dmax, int32_t* om,
+                      int64_t* oe, int64_t oplane, void* stream);
+
 /* digit matrices of C (as b3d_rns_split writes them) from table[(d + dmax) * np + j] = residues of
  * round(2^(NB-1) / d) */
 int b3d_cauchy_digits(const b3d_level_tables* lv, const uint32_t* table, int64_t dmax, int np, int64_t Rp, int64_t Kp,

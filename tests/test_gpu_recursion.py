@@ -87,7 +87,7 @@ def test_recursion_golden_operators(cuda, ci, cauchy):
     (3, 1, 5, 6, ((0, 1), (1, 1)), 18, 2, 13),
     (2, 2, 6, 8, ((0, 0), (1, 1)), 34, 1, 14),
 ])
-@pytest.mark.parametrize("cauchy", ["cuda", "rns"])
+@pytest.mark.parametrize("cauchy", ["cuda", "cuda3", "rns"])
 def test_recursion_random_operators(cuda, case, cauchy):
     tj12, tj43, tjmax, order, pp, L, nrhs, seed = case
     M, H = random_case(*case)
@@ -113,16 +113,18 @@ def test_slot_reuse_same_live_residues(cuda):
 
 
 @pytest.mark.parametrize("case", [
-    (4, 2, 6, 9, ((0, 1), (1, 0)), 10, 3, 61),
+    (4, 2, 6, 9, ((0, 1), (1, 0)), 10, 3, 61),              # divisors < 2^8: 24-bit digits in cuda3
     (8, 8, 6, 8, ((0, 0), (1, 1)), 34, 2, 62),
+    (2, 2, 60, 50, ((0, 0), (1, 1)), 10, 1, 63),            # divisors up to 314: 22-bit digits in cuda3
 ])
 def test_cauchy_forms_bitwise_equal(cuda, case):
-    """the pre-aligned two-terms-per-thread Cauchy kernel gives the first kernel's bits"""
+    """the pre-aligned two-terms-per-thread Cauchy kernel and its wide-digit form give the first kernel's bits"""
     tj12, tj43, tjmax, order, pp, L, nrhs, seed = case
     M, H = random_case(*case)
     plan = PL.Plan(tj12, tj43, tjmax, order, pp, reuse=True)
     outs = []
-    for form in ("cuda", "cuda2"):
+    for form in ("cuda", "cuda2", "cuda3"):
         rec = RC.Recursion(plan, M, L, device=cuda, cauchy=form)
         outs.append(rec.run(hinf_tensor(H, plan, order, nrhs, L, cuda)))
-    assert torch.equal(outs[0].m, outs[1].m) and torch.equal(outs[0].e, outs[1].e)
+    for o in outs[1:]:
+        assert torch.equal(outs[0].m, o.m) and torch.equal(outs[0].e, o.e)
