@@ -302,6 +302,161 @@ __global__ void __launch_bounds__(128, 1) k_rns_mma(RnsMma a, RnsTables tb) {
 }
 #endif
 
+#ifdef B3D_RNS_MMA
+// 2''. the product with the CRT-operand epilogue, four primes per CTA.  256 threads: thread 0 issues the bulk
+// copies (double-buffered: the operands of prime j + 1 arrive while prime j is multiplied and reduced) and
+// the MMAs; both warpgroups read TMEM (warp w reads lanes 32 (w % 4), warpgroup h the h-th half of the
+// column chunks) and reduce.  The y bytes of the four primes of an output are staged in shared memory and
+// leave as one 16-byte store per output (columns 16 g .. 16 g + 15 of the CRT operand).
+constexpr int kPrimesPerCta = 4;
+
+__global__ void __launch_bounds__(256, 1) k_rns_mma4(RnsMma a, RnsTables tb) {
+    extern __shared__ __align__(128) uint8_t smem[];
+    __shared__ __align__(8) uint64_t bar_load[2], bar_mma;
+    __shared__ uint32_t tmem_base_sh;
+    __shared__ int fail_sh;
+
+    const int TN = a.TN, Kp = a.Kp, np = tb.np;
+    const int64_t g = blockIdx.z, b = blockIdx.y;
+    const int64_t ti = blockIdx.x / a.tiles_l, tl = blockIdx.x % a.tiles_l;
+    const uint32_t xbytes = 128u * Kp, ybytes = (uint32_t)TN * Kp, stage = xbytes + ybytes;
+    uint8_t* ysm = smem + 2 * (size_t)stage;             // (32 rows i x TN / 4 columns l) x 16 bytes
+    const int warp = threadIdx.x / 32;
+    const int j0 = (int)g * kPrimesPerCta;
+    const int nj = np - j0 < kPrimesPerCta ? np - j0 : kPrimesPerCta;
+    uint32_t ncols = 32;
+    while (ncols < (uint32_t)TN) ncols <<= 1;
+
+    if (threadIdx.x == 0) {
+        fail_sh = 0;
+        mbar_init(&bar_load[0], 1);
+        mbar_init(&bar_load[1], 1);
+        mbar_init(&bar_mma, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                     ::"r"(smem_u32(&tmem_base_sh)), "r"(ncols) : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = tmem_base_sh;
+
+    int issued = 0, waited = 0, mma_pending = 0;         // thread 0's bookkeeping (for the failure drain)
+    if (threadIdx.x == 0) {
+        const uint8_t* gx = a.X + (size_t)((int64_t)j0 * a.nb + b) * a.x_mat + (size_t)ti * xbytes;
+        const uint8_t* gy = a.Y + (size_t)((int64_t)j0 * a.nb + b) * a.y_mat + (size_t)tl * ybytes;
+        mbar_expect_tx(&bar_load[0], stage);
+        bulk_copy_g2s(smem, gx, xbytes, &bar_load[0]);
+        bulk_copy_g2s(smem + xbytes, gy, ybytes, &bar_load[0]);
+        issued = 1;
+    }
+    const int row = threadIdx.x & 127, s = row & 3, half = threadIdx.x >> 7;
+    const uint32_t taddr = tmem + ((uint32_t)((warp & 3) * 32) << 16);
+    const int chunks = TN / 16, c_lo = half ? (chunks + 1) / 2 : 0, c_hi = half ? chunks : (chunks + 1) / 2;
+    const uint32_t idesc = (2u << 4) | ((uint32_t)(TN >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+
+    for (int pi = 0; pi < nj; pi++) {
+        const int j = j0 + pi;
+        const int buf = pi & 1;
+        if (threadIdx.x == 0 && pi + 1 < nj) {           // prefetch prime j + 1 into the other buffer
+            const uint8_t* gx = a.X + (size_t)((int64_t)(j + 1) * a.nb + b) * a.x_mat + (size_t)ti * xbytes;
+            const uint8_t* gy = a.Y + (size_t)((int64_t)(j + 1) * a.nb + b) * a.y_mat + (size_t)tl * ybytes;
+            uint8_t* dst = smem + (size_t)(buf ^ 1) * stage;
+            mbar_expect_tx(&bar_load[buf ^ 1], stage);
+            bulk_copy_g2s(dst, gx, xbytes, &bar_load[buf ^ 1]);
+            bulk_copy_g2s(dst + xbytes, gy, ybytes, &bar_load[buf ^ 1]);
+            issued = pi + 2;
+        }
+        if (!mbar_wait(&bar_load[buf], (pi >> 1) & 1, kWaitLimit)) atomicExch(&fail_sh, 1);
+        else if (threadIdx.x == 0) waited = pi + 1;
+        __syncthreads();
+        if (fail_sh) break;
+        if (threadIdx.x == 0) {
+            const uint32_t ax = smem_u32(smem + (size_t)buf * stage), ay = ax + xbytes;
+            for (int kk = 0; kk < Kp / 32; kk++) {
+                uint64_t da = umma_desc(ax + kk * 2 * (128 * 16), 128 * 16, 128);
+                uint64_t db = umma_desc(ay + kk * 2 * (TN * 16), TN * 16, 128);
+                uint32_t acc = kk > 0 ? 1u : 0u;
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\t"
+                    "setp.ne.b32 p, %4, 0;\n\t"
+                    "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}"
+                    ::"r"(tmem), "l"(da), "l"(db), "r"(idesc), "r"(acc) : "memory");
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                         ::"r"(smem_u32(&bar_mma)) : "memory");
+            mma_pending = 1;
+        }
+        if (!mbar_wait(&bar_mma, pi & 1, kWaitLimit)) atomicExch(&fail_sh, 2);
+        else if (threadIdx.x == 0) mma_pending = 0;
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        __syncthreads();
+        if (fail_sh) break;
+
+        const uint32_t p = __ldg(tb.p + j);
+        const uint64_t mu = __ldg(tb.mu + j);
+        const uint32_t inv = __ldg(tb.inv + j);
+        uint32_t w[7];
+#pragma unroll
+        for (int u = 0; u < 7; u++) w[u] = __ldg(tb.w + j * 8 + u);
+        for (int c = c_lo; c < c_hi; c++) {
+            const int c0 = 16 * c;
+            uint32_t d[16];
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+                "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
+                : "=r"(d[0]), "=r"(d[1]), "=r"(d[2]), "=r"(d[3]), "=r"(d[4]), "=r"(d[5]), "=r"(d[6]), "=r"(d[7]),
+                  "=r"(d[8]), "=r"(d[9]), "=r"(d[10]), "=r"(d[11]), "=r"(d[12]), "=r"(d[13]), "=r"(d[14]), "=r"(d[15])
+                : "r"(taddr + (uint32_t)c0));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                uint64_t v = 0;
+#pragma unroll
+                for (int t = 0; t < 4; t++) v += (uint64_t)d[4 * q + t] * w[s + t];
+                v += __shfl_xor_sync(0xFFFFFFFFu, v, 1);
+                v += __shfl_xor_sync(0xFFFFFFFFu, v, 2);
+                if (s == 0) {
+                    const uint32_t r = barrett(v, p, mu);
+                    const uint32_t y = barrett((uint64_t)r * inv, p, mu);
+                    const int ll = c0 / 4 + q;
+                    *reinterpret_cast<uint32_t*>(ysm + ((size_t)(row >> 2) * (TN / 4) + ll) * 16 + 4 * pi) = y;
+                }
+            }
+        }
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncthreads();                                  // TMEM read out before the next prime's MMAs
+    }
+    if (!fail_sh) {                                       // one 16-byte store per output
+        const int nl = TN / 4, per = 32 * nl;
+        const bool lfast = a.out_l == 1;
+        for (int x = threadIdx.x; x < per; x += blockDim.x) {
+            const int il = lfast ? x / nl : x % 32, ll = lfast ? x % nl : x / 32;
+            const int64_t ii = ti * 32 + il, l = tl * nl + ll;
+            if (ii < a.NI && l < a.NL) {
+                const int64_t e = b * a.out_b + ii * a.out_i + l * a.out_l;
+                *reinterpret_cast<uint4*>(a.yb + tiled_offset(e, 4 * (int64_t)j0, 128, a.crt_kp)) =
+                    *reinterpret_cast<const uint4*>(ysm + ((size_t)il * nl + ll) * 16);
+            }
+        }
+    }
+    if (threadIdx.x == 0 && fail_sh) {                    // bounded drain of our own copies and MMAs
+        for (int q = waited; q < issued; q++)
+            if (!mbar_wait(&bar_load[q & 1], (q >> 1) & 1, kWaitLimit)) { fail_sh = 3; break; }
+        if (fail_sh != 3 && mma_pending && !mbar_wait(&bar_mma, (waited - 1) & 1, kWaitLimit)) fail_sh = 4;
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncols) : "memory");
+    }
+    if (threadIdx.x == 0 && fail_sh) atomicExch(a.err, fail_sh);
+}
+#endif
+
 // ------------------------------------------------------------------------------------------------
 // 1'. digits on the tensor cores.  One CTA = a tile of 8 operand rows x 16 columns k (128 elements).  The
 // elements' magnitude bytes form A (128 rows x 4 L bytes, K-major in shared memory); the constant
