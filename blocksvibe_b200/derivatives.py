@@ -127,6 +127,7 @@ class Derivs:
         # index tensors of finish_iter, built once (no host-to-device copies while a CUDA graph is captured)
         self._jidx = torch.tensor([(tj - tj12 % 2) // 2 for tj in self.tjs], device=self.device)
         self._orders = {}
+        self._acache = {}                  # row-aligned constant GEMM operands (shared by the for_order copies)
 
     # ------------------------------------------------------------ moment bookkeeping per level
     def _moment_levels(self):
@@ -298,7 +299,8 @@ class Derivs:
         jidx = self._jidx
         H = MPF(h_inf.m[:, :, :order + 1][:, :, :, jidx], h_inf.e[:, :order + 1][:, :, jidx])   # (2, o+1, Jo, S2, B)
         H = H.permute(1, 2, 0, 3, 4).contiguous().reshape(order + 1, Jo * Nc)
-        c = mpf.gemm(self.Wh, H).reshape(R1, Jo, Nc).permute(1, 0, 2)                          # (Jo, R+1, Nc)
+        ac = self._acache
+        c = mpf.gemm(self.Wh, H, cache=ac, key=("Wh", R)).reshape(R1, Jo, Nc).permute(1, 0, 2)  # (Jo, R+1, Nc)
         mom = self.mom.reshape(2, Jo, NP, R1, N)
         chunk = chunk or Jo
         for j0 in range(0, Jo, chunk):
@@ -306,14 +308,19 @@ class Derivs:
             J = j1 - j0
             v = mom[:, j0:j1].permute(1, 2, 3, 0, 4).contiguous().reshape(J, NP, R1, Nc)           # v_i[d]
             di = self.didx[j0:j1].reshape(-1)
-            a = mpf.gemm(self.Ttab, v.reshape(J * NP, R1, Nc), aidx=di).reshape(J, NP, R1, Nc)    # a_i[e]
-            T = self.Ttab.take(di).reshape(J, NP, R1, R1)                                          # [.., w, 0] = D_i^w
-            Vand = MPF(T.m[:, :, :, :Rw, 0].permute(0, 1, 3, 2), T.e[:, :, :Rw, 0].permute(0, 2, 1)).contiguous()
-            G = mpf.gemm(Vand, v.reshape(J, NP, R1 * Nc)).reshape(J, Rw * R1, Nc)                # G[w][d]
+            a = mpf.gemm(self.Ttab, v.reshape(J * NP, R1, Nc), aidx=di, cache=ac,
+                         key=("Ttab", R, j0, j1)).reshape(J, NP, R1, Nc)                            # a_i[e]
+            vkey = ("Vand", R, j0, j1)
+            if (vkey, J) not in ac:
+                T = self.Ttab.take(di).reshape(J, NP, R1, R1)                                      # [.., w, 0] = D_i^w
+                Vand = MPF(T.m[:, :, :, :Rw, 0].permute(0, 1, 3, 2), T.e[:, :, :Rw, 0].permute(0, 2, 1)).contiguous()
+            else:
+                Vand = None
+            G = mpf.gemm(Vand, v.reshape(J, NP, R1 * Nc), cache=ac, key=vkey).reshape(J, Rw * R1, Nc)  # G[w][d]
             Gz = mpf.cat([G, mpf.zeros((J, 1, Nc), L, dev)], 1)
             Gs = Gz.permute(1, 0, 2).contiguous().take(self.gidx).reshape(R1, R1, J, Nc)          # (s, d, jo, col)
             Gs = Gs.permute(1, 2, 0, 3).contiguous().reshape(R1, J * R1 * Nc)                     # (d, jo s col)
-            Hm = mpf.gemm(self.Cb, Gs).reshape(R1, J, R1, Nc)                                     # H[e][s]
+            Hm = mpf.gemm(self.Cb, Gs, cache=ac, key=("Cb", R)).reshape(R1, J, R1, Nc)           # H[e][s]
             Hm = mpf.cat([Hm.permute(0, 2, 1, 3).contiguous().reshape(R1 * R1, J, Nc),
                           mpf.zeros((1, J, Nc), L, dev)], 0)
             cz = mpf.cat([c[j0:j1].permute(1, 0, 2).contiguous(), mpf.zeros((1, J, Nc), L, dev)], 0)  # (d | 0, jo, col)
@@ -326,5 +333,5 @@ class Derivs:
             P = mpf.add(P, Hm.take(self.hidx_te).contiguous())                                    # ((t, e), jo, col)
             P = P.reshape(R1, R1, J, Nc).permute(2, 0, 1, 3).contiguous().reshape(J, R1, R1 * Nc)  # (jo, t, e col)
             Bn = mpf.cat([a.reshape(J, NP, R1 * Nc), P], 1)                                       # (jo, i | t, e col)
-            num = mpf.gemm(self.Anum[j0:j1], Bn)                                                  # (J, Dout, R+1 Nc)
+            num = mpf.gemm(self.Anum[j0:j1], Bn, cache=ac, key=("Anum", R, j0, j1))               # (J, Dout, R+1 Nc)
             yield j0, num.reshape(J, self.Dout, R1, 2, S2, self.B)

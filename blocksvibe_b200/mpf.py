@@ -266,15 +266,23 @@ def _use_rns(K):
     return GEMM_BACKEND == "rns" or K >= RNS_MIN_K
 
 
-def gemm(A, B, aidx=None):
+def gemm(A, B, aidx=None, cache=None, key=None):
     """multiprecision (batched) product with the semantics of the reference's mpf.gemm (A aligned per row,
     B per column, exact products, one rounding per entry; reference ``recursion_gpu.py:53-79``).
-    A: (M, K), (nb, M, K), or a table gathered by aidx (nb); B: (K, N) or (nb, K, N)."""
-    _check(A, B)
+    A: (M, K), (nb, M, K), or a table gathered by aidx (nb); B: (K, N) or (nb, K, N).
+    cache / key: for a constant A (the caller's promise), its row-aligned form is kept in cache[(key, nb)]
+    and reused by later calls."""
     batched = len(B.shape) == 3
     Bb = B if batched else B.reshape(1, *B.shape)
     nb = Bb.shape[0]
-    if aidx is not None:
+    ck = (key, nb) if cache is not None and key is not None else None
+    if A is None and (ck is None or ck not in cache):
+        raise ValueError("gemm: A is None and not cached")
+    _check(*((A, B) if A is not None else (B,)))
+    Aal = cache.get(ck) if ck is not None else None
+    if Aal is not None:
+        pass
+    elif aidx is not None:
         Aal = align_rows(A, bidx=aidx)
     elif len(A.shape) == 2:
         Aal = align_rows(A.reshape(1, *A.shape))
@@ -282,6 +290,8 @@ def gemm(A, B, aidx=None):
             Aal = (Aal[0].expand(-1, nb, -1, -1).contiguous(), Aal[1].expand(nb, -1).contiguous())
     else:
         Aal = align_rows(A)
+    if ck is not None and ck not in cache:
+        cache[ck] = Aal
     Bal = align_cols(Bb)
     if _use_rns(Aal[0].shape[-1]):
         from .rns import gemm_aligned_rns

@@ -180,6 +180,7 @@ class Output:
                 raise ValueError(f"coordinate {coordinate!r}: only xt and xt_radial")
         self.nL = (Lam - parity) // 2 + 1
         self._idx = {}                     # cached index tensors (no host copies while a CUDA graph is captured)
+        self._acache = {}                  # the row-aligned map W per batch size
         self.Wmp = W
         self.W = mpf.from_mp(list(W.reshape(-1)), L, W.shape, device)
 
@@ -195,7 +196,7 @@ class Output:
             self._idx[key] = torch.tensor([e * nL + i for i, e in self.inputs], device=num.device)
         uidx = self._idx[key]
         X = X.reshape(R1 * nL, -1).take(uidx)
-        out = mpf.gemm(self.W, X).reshape(len(self.outputs), Jo, 2, S2, nq, Dout)
+        out = mpf.gemm(self.W, X, cache=self._acache, key="W").reshape(len(self.outputs), Jo, 2, S2, nq, Dout)
         return out.permute(1, 2, 3, 4, 0, 5).contiguous()
 
 
@@ -219,5 +220,5 @@ def apply_per_order(out, nums):
         rows.append(X.reshape(R1, -1).take(out._idx[key]))
     X = mpf.cat(rows, 0)
     Jo, _, _, _, S2, nq = nums[0].shape
-    res = mpf.gemm(out.W, X).reshape(len(out.outputs), Jo, 2, S2, nq, Dmax)
+    res = mpf.gemm(out.W, X, cache=out._acache, key="W").reshape(len(out.outputs), Jo, 2, S2, nq, Dmax)
     return res.permute(1, 2, 3, 4, 0, 5).contiguous()
