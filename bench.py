@@ -41,6 +41,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--sample", type=int, default=12, help="set644: number of task groups timed")
     ap.add_argument("--no-graph", action="store_true", help="launch every kernel from Python instead of a CUDA graph")
+    ap.add_argument("--rate", type=float, default=2.0, help="cfg4: Poisson arrival rate (tasks/s)")
+    ap.add_argument("--requests", type=int, default=32, help="cfg4: requests in the stream")
     return ap.parse_args()
 
 
@@ -521,6 +523,32 @@ def run_set(args):
         s1.record()
         torch.cuda.synchronize()
         out[name] = max_over_ranks(s0.elapsed_time(s1) / args.steps, world, dev)
+    # the same tasks through the serving loop: all submitted at once, continuous batching per operator, two
+    # workers on their own streams, results left on the device for the GPU JSON writer (wall clock from the
+    # first submit to the last result)
+    from blocksvibe_b200 import serve
+    srv = serve.Server(dev, workers=2, max_batch=32, host_results=False)
+    for op, tasks, ns, d12 in prepared:
+        srv.add_operator(op, op.group, tasks[0])
+    try:
+        warm = [srv.submit(op.group, tasks[0], None) for op, tasks, ns, d12 in prepared]
+        for r in warm:
+            srv.wait(r, timeout=900)
+        n0, nb0 = len(srv.finished), len(srv.batches)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        reqs = [srv.submit(op.group, t, None) for op, tasks, ns, d12 in prepared for t in tasks]
+        for r in reqs:
+            srv.wait(r, timeout=1800)
+        serve_s = time.perf_counter() - t0
+        lat = sorted(r.done - r.arrival for r in srv.finished[n0:])
+    finally:
+        srv.close()
+    serving = {"value": ntask / serve_s, "unit": "tasks/s", "wall_s": serve_s, "requests": len(reqs),
+               "batches": len(srv.batches) - nb0,
+               "latency_ms": {"p50": serve.percentile(lat, 0.5) * 1e3, "p99": serve.percentile(lat, 0.99) * 1e3},
+               "includes": "results left on the device for the GPU JSON writer (wall clock)",
+               "over_plain": (ntask / serve_s) / (ntask / (out["plain"] / 1e3))}
     if rank == 0:
         line = {"metric": "blocks_3d tasks/s", "value": world * ntask / (out["batched"] / 1e3), "unit": "tasks/s",
                 "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": out["batched"],
@@ -529,7 +557,58 @@ def run_set(args):
                 "config": {"workload": "set644", "groups": len(picked), "tasks": ntask,
                            "group_sizes": [n for _, n in picked]},
                 "plain": {"value": world * ntask / (out["plain"] / 1e3), "ms_per_step": out["plain"]},
-                "batched_over_plain": out["plain"] / out["batched"], "setup_s": setup_s}
+                "batched_over_plain": out["plain"] / out["batched"], "serving_loop": serving, "setup_s": setup_s}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def run_stream(args):
+    """--workload cfg4: a Poisson stream of config-2-shaped tasks (mixed precision 512 / 768 / 1024 / 1280 bits,
+    pole shifting on for half of them: kept pole order 20 or none) through the serving loop at --rate tasks/s;
+    operators are built before the stream starts.  Reports achieved tasks/s and p50 / p99 latency."""
+    import random
+    import torch
+    from blocksvibe_b200 import dropin as DI, serve
+    from blocksvibe_b200.workloads import CONFIGS, make_device_tasks
+    world, rank, local = dist_setup()
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    kinds = [dict(CONFIGS["cfg2"], precision=p, kept=k) for p in (512, 768, 1024, 1280) for k in (20, 40)]
+    per = max(1, (args.requests + len(kinds) - 1) // len(kinds))
+    srv = serve.Server(dev, workers=2, max_batch=16)
+    pools = []
+    t0 = time.perf_counter()
+    for ki, c in enumerate(kinds):
+        G, tasks = make_device_tasks(c, per, dev, seed=100 + ki)
+        t = tasks[0]
+        op = DI.Operator(G, t.pp, t.parity, None, t.two_js_internal, list(t.coordinates), [t.delta_1_plus_2], dev)
+        op.apply_outputs(op.run_batched(tasks[:1], t.lambda_orders(G.Lambda)), t.delta_1_plus_2)   # warm
+        srv.add_operator(op, G, t)
+        pools.append((G, tasks))
+    torch.cuda.synchronize()
+    setup_s = time.perf_counter() - t0
+    rng = random.Random(4)
+    items = []
+    for i in range(args.requests):
+        G, tasks = pools[rng.randrange(len(pools))]
+        items.append((G, tasks[i % len(tasks)], None))
+    try:
+        reqs, wall = serve.replay(srv, items, args.rate, seed=5)
+    finally:
+        srv.close()
+    lat = sorted(r.done - r.arrival for r in reqs)
+    if rank == 0:
+        line = {"metric": "blocks_3d tasks/s", "value": len(reqs) / wall, "unit": "tasks/s", "n_gpus": world,
+                "steps": len(reqs), "warmup": len(kinds), "ms_per_step": wall / len(reqs) * 1e3,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "mpf int32 limbs",
+                "data": "synthetic (Poisson stream of random config-2-shaped tasks)",
+                "config": {"workload": "cfg4", "arrival_rate": args.rate, "requests": len(reqs),
+                           "precisions": [512, 768, 1024, 1280], "pole_shifting": "half (kept 20 or off)",
+                           "results": "copied to host (pinned)"},
+                "latency_ms": {"p50": serve.percentile(lat, 0.5) * 1e3, "p99": serve.percentile(lat, 0.99) * 1e3},
+                "batches": len(srv.batches), "peak_in_flight_bytes": srv.peak_in_flight, "setup_s": setup_s}
         print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as dist
@@ -542,6 +621,8 @@ def main():
         run_reference(args)
     elif args.workload == "set644":
         run_set(args)
+    elif args.workload == "cfg4":
+        run_stream(args)
     else:
         run_ours(args)
 

@@ -260,10 +260,15 @@ GEMM_BACKEND = "auto"
 RNS_MIN_K = 32
 
 
-def _use_rns(K):
+RNS_MIN_K_WIDE, RNS_WIDE = 16, 4096
+
+
+def _use_rns(K, M=0, N=0):
+    """the residue GEMM pays for its digit split and CRT when K is large, or when K is moderate and one side
+    of the (per batch) product is wide enough to fill the tensor-core tiles"""
     if GEMM_BACKEND == "schoolbook" or K > 256:
         return False
-    return GEMM_BACKEND == "rns" or K >= RNS_MIN_K
+    return GEMM_BACKEND == "rns" or K >= RNS_MIN_K or (K >= RNS_MIN_K_WIDE and max(M, N) >= RNS_WIDE)
 
 
 def gemm(A, B, aidx=None, cache=None, key=None):
@@ -293,7 +298,7 @@ def gemm(A, B, aidx=None, cache=None, key=None):
     if ck is not None and ck not in cache:
         cache[ck] = Aal
     Bal = align_cols(Bb)
-    if _use_rns(Aal[0].shape[-1]):
+    if _use_rns(Aal[0].shape[-1], Aal[0].shape[-2], Bal[0].shape[-1]):
         from .rns import gemm_aligned_rns
         C = gemm_aligned_rns(Aal, Bal)
     else:

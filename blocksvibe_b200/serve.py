@@ -43,8 +43,12 @@ def operator_key(group, task):
 
 
 class Server:
-    def __init__(self, device="cuda", budget_bytes=None, workers=2, max_batch=32, schedule="batched"):
+    def __init__(self, device="cuda", budget_bytes=None, workers=2, max_batch=32, schedule="batched",
+                 host_results=True):
+        """host_results: copy each result to host arrays (the reference's cli._gpu contract); False keeps it on
+        the device as MPF views of the batch output (for the GPU JSON writer, jsonout.SpinWriter)"""
         self.device = torch.device(device)
+        self.host_results = host_results
         if budget_bytes is None:
             free, _ = torch.cuda.mem_get_info(self.device)
             budget_bytes = int(0.5 * free)
@@ -66,6 +70,12 @@ class Server:
             th.start()
 
     # ------------------------------------------------------------ client side
+    def add_operator(self, op, group, task):
+        """register an operator built elsewhere (dropin.Operator) for the requests of (group, task)'s key"""
+        with self.lock:
+            self.ops[operator_key(group, task)] = op
+            self.lock.notify_all()
+
     def submit(self, group, task, M, arrival=None):
         with self.lock:
             r = Request(group, task, M, time.perf_counter() if arrival is None else arrival, self.next_id)
@@ -180,12 +190,22 @@ class Server:
                     tasks = [r.task for r in batch]
                     nums = op.run_batched(tasks, ns) if self.schedule == "batched" else op.run_plain(tasks, ns)
                     out = op.apply_outputs(nums, head.task.delta_1_plus_2)
-                    host = {c: (r.m.cpu(), r.e.cpu()) for c, r in out.items()}
+                    if self.host_results:                  # pinned buffers: one asynchronous copy per array
+                        host = {}
+                        for c, x in out.items():
+                            hm = torch.empty(x.m.shape, dtype=torch.int32, pin_memory=True)
+                            he = torch.empty(x.e.shape, dtype=torch.int64, pin_memory=True)
+                            hm.copy_(x.m, non_blocking=True)
+                            he.copy_(x.e, non_blocking=True)
+                            host[c] = (hm, he)
                     stream.synchronize()
                 now = time.perf_counter()
+                d12 = head.task.delta_1_plus_2
                 for q, r in enumerate(batch):
-                    r.result = {(c, head.task.delta_1_plus_2): (m[:, :, :, :, q].numpy(), e[:, :, :, q].numpy())
-                                for c, (m, e) in host.items()}
+                    if self.host_results:
+                        r.result = {(c, d12): (m[:, :, :, :, q].numpy(), e[:, :, :, q].numpy()) for c, (m, e) in host.items()}
+                    else:
+                        r.result = {(c, d12): x[:, :, :, q:q + 1] for c, x in out.items()}
                     r.done = now
             except Exception as exc:                           # surfaced to the waiting client
                 for r in batch:

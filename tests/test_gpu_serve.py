@@ -46,3 +46,22 @@ def test_poisson_replay_reports_latency(cuda):
     lat = [r.done - r.arrival for r in reqs]
     assert serve.percentile(lat, 0.5) <= serve.percentile(lat, 0.99)
     assert elapsed > 0 and all(r.result for r in reqs)
+
+
+def test_device_resident_results_equal_host_results(cuda):
+    """host_results=False leaves each result on the GPU (for the GPU JSON writer): same values"""
+    G, tasks, M, _, _ = make_group(nq=3, seed=24, coords=("xt",), d12="2.3")
+    out = {}
+    for host in (True, False):
+        srv = serve.Server(cuda, workers=2, max_batch=8, host_results=host)
+        try:
+            reqs = [srv.submit(G, t, M) for t in tasks]
+            for r in reqs:
+                srv.wait(r, timeout=600)
+        finally:
+            srv.close()
+        out[host] = [r.result for r in reqs]
+    for a, b in zip(out[True], out[False]):
+        for key, (m, e) in a.items():
+            x = b[key]
+            assert np.array_equal(m, x.m.cpu().numpy()[:, :, :, :, 0]) and np.array_equal(e, x.e.cpu().numpy()[:, :, :, 0])
