@@ -412,20 +412,26 @@ __global__ void __launch_bounds__(256, 1) k_rns_mma4(RnsMma a, RnsTables tb) {
                   "=r"(d[8]), "=r"(d[9]), "=r"(d[10]), "=r"(d[11]), "=r"(d[12]), "=r"(d[13]), "=r"(d[14]), "=r"(d[15])
                 : "r"(taddr + (uint32_t)c0));
             asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            // partial sums of the four outputs q of this chunk (this lane's row digit s), then a
+            // reduce-scatter over the four lanes of the row: lane s ends with the full sum of output q = s
+            uint64_t pq[4];
 #pragma unroll
             for (int q = 0; q < 4; q++) {
                 uint64_t v = 0;
 #pragma unroll
                 for (int t = 0; t < 4; t++) v += (uint64_t)d[4 * q + t] * w[s + t];
-                v += __shfl_xor_sync(0xFFFFFFFFu, v, 1);
-                v += __shfl_xor_sync(0xFFFFFFFFu, v, 2);
-                if (s == 0) {
-                    const uint32_t r = barrett(v, p, mu);
-                    const uint32_t y = barrett((uint64_t)r * inv, p, mu);
-                    const int ll = c0 / 4 + q;
-                    *reinterpret_cast<uint32_t*>(ysm + ((size_t)(row >> 2) * (TN / 4) + ll) * 16 + 4 * pi) = y;
-                }
+                pq[q] = v;
             }
+            const bool hi2 = (s & 2) != 0, hi1 = (s & 1) != 0;
+            const uint64_t k0 = hi2 ? pq[2] : pq[0], k1 = hi2 ? pq[3] : pq[1];
+            const uint64_t x0 = hi2 ? pq[0] : pq[2], x1 = hi2 ? pq[1] : pq[3];
+            const uint64_t a0 = k0 + __shfl_xor_sync(0xFFFFFFFFu, x0, 2);     // outputs (s & 2) + {0, 1}
+            const uint64_t a1 = k1 + __shfl_xor_sync(0xFFFFFFFFu, x1, 2);
+            const uint64_t v = (hi1 ? a1 : a0) + __shfl_xor_sync(0xFFFFFFFFu, hi1 ? a0 : a1, 1);   // output s
+            const uint32_t r = barrett(v, p, mu);
+            const uint32_t y = barrett((uint64_t)r * inv, p, mu);
+            const int ll = c0 / 4 + s;
+            *reinterpret_cast<uint32_t*>(ysm + ((size_t)(row >> 2) * (TN / 4) + ll) * 16 + 4 * pi) = y;
         }
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
         __syncthreads();                                  // TMEM read out before the next prime's MMAs
