@@ -122,7 +122,7 @@ class Clocks:
 
 
 # ---------------------------------------------------------------- kernel probe (launch count, per-kernel events)
-KERNELS_PER_CALL = {"b3d_pole_level": 2}
+KERNELS_PER_CALL = {"b3d_pole_level": 2, "b3d_cauchy_align": 2}
 
 
 class Probe:

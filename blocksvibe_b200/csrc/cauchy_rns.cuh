@@ -10,10 +10,12 @@
 
 namespace b3d {
 
-// X[g][i][n] (layout (nb, Kc, N)) aligned to the column's largest exponent, column exponents oe[g * N + n]
+// X[g][i][n] (layout (nb, Kc, N)) aligned to the column's largest exponent, column exponents oe[g * N + n].
+// Two kernels: the exponent of each column (g, n), then one thread per element (g, i, n) for the shifts, so
+// that a level's nb Kc N elements spread over the whole GPU (consecutive threads: consecutive n, coalesced).
 template <int L>
-__global__ void k_cauchy_align(const int32_t* __restrict__ rm, const i64* __restrict__ re, i64 rplane, CauchyLevel lv,
-                               int32_t* __restrict__ om, i64* __restrict__ oe, i64 oplane) {
+__global__ void k_cauchy_colexp(const int32_t* __restrict__ rm, const i64* __restrict__ re, i64 rplane, CauchyLevel lv,
+                                i64* __restrict__ oe) {
     i64 t = blockIdx.x * (i64)blockDim.x + threadIdx.x;
     const i64 N = lv.N;
     if (t >= lv.nb * N) return;
@@ -27,21 +29,28 @@ __global__ void k_cauchy_align(const int32_t* __restrict__ rm, const i64* __rest
         if (ei > E && rm[(L - 1) * rplane + ix] != 0) E = ei;
     }
     oe[t] = E;
-    for (i64 i = 0; i < lv.Kc; i++) {
-        const i64 dst = (g * lv.Kc + i) * N + n;
-        u32 a[L], s[L];
-        bool neg = false;
-        if (i < ncol && E != EZ) {
-            const i64 ix = col[i] * N + n;
-            neg = load_mag<L>(rm, rplane, ix, a);
-            const i64 ei = re[ix];
-            if (is_zero(a) || ei == EZ || E - ei >= 32 * L) { zero(s); neg = false; }
-            else shr(a, (int)(E - ei), s);
-        } else {
-            zero(s);
-        }
-        store_signed<L>(om, oplane, dst, s, neg);
+}
+
+template <int L>
+__global__ void k_cauchy_align(const int32_t* __restrict__ rm, const i64* __restrict__ re, i64 rplane, CauchyLevel lv,
+                               const i64* __restrict__ ce, int32_t* __restrict__ om, i64 oplane) {
+    i64 t = blockIdx.x * (i64)blockDim.x + threadIdx.x;
+    const i64 N = lv.N;
+    if (t >= lv.nb * lv.Kc * N) return;
+    const i64 n = t % N, i = (t / N) % lv.Kc, g = t / (N * lv.Kc);
+    const i64 E = ce[g * N + n];
+    u32 a[L], s[L];
+    bool neg = false;
+    if (i < lv.ncol[g] && E != EZ) {
+        const i64 ix = lv.col[g * lv.Kc + i] * N + n;
+        neg = load_mag<L>(rm, rplane, ix, a);
+        const i64 ei = re[ix];
+        if (is_zero(a) || ei == EZ || E - ei >= 32 * L) { zero(s); neg = false; }
+        else shr(a, (int)(E - ei), s);
+    } else {
+        zero(s);
     }
+    store_signed<L>(om, oplane, t, s, neg);
 }
 
 #ifdef B3D_RNS_MMA
@@ -119,9 +128,10 @@ struct CauchyRnsLaunch {
 template <int L>
 int CauchyRnsLaunch<L>::align(const int32_t* rm, const i64* re, i64 rplane, const CauchyLevel& lv, int32_t* om,
                               i64* oe, i64 oplane, cudaStream_t st) {
-    const i64 n = lv.nb * lv.N;
+    const i64 n = lv.nb * lv.N, ne = n * lv.Kc;
     if (n == 0) return 0;
-    k_cauchy_align<L><<<(unsigned)((n + 127) / 128), 128, 0, st>>>(rm, re, rplane, lv, om, oe, oplane);
+    k_cauchy_colexp<L><<<(unsigned)((n + 127) / 128), 128, 0, st>>>(rm, re, rplane, lv, oe);
+    if (ne > 0) k_cauchy_align<L><<<(unsigned)((ne + 127) / 128), 128, 0, st>>>(rm, re, rplane, lv, oe, om, oplane);
     return (int)cudaGetLastError();
 }
 
