@@ -304,15 +304,15 @@ __global__ void __launch_bounds__(128, 1) k_rns_mma(RnsMma a, RnsTables tb) {
 
 #ifdef B3D_RNS_MMA
 // 2''. the product with the CRT-operand epilogue, four primes per CTA.  256 threads: thread 0 issues the bulk
-// copies (double-buffered: the operands of prime j + 1 arrive while prime j is multiplied and reduced) and
-// the MMAs; both warpgroups read TMEM (warp w reads lanes 32 (w % 4), warpgroup h the h-th half of the
+// copies (one operand buffer: as soon as the MMAs of prime j have completed, the operands of prime j + 1
+// are copied into it while the epilogue of prime j runs) and the MMAs; both warpgroups read TMEM (warp w reads lanes 32 (w % 4), warpgroup h the h-th half of the
 // column chunks) and reduce.  The y bytes of the four primes of an output are staged in shared memory and
 // leave as one 16-byte store per output (columns 16 g .. 16 g + 15 of the CRT operand).
 constexpr int kPrimesPerCta = 4;
 
-__global__ void __launch_bounds__(256, 1) k_rns_mma4(RnsMma a, RnsTables tb) {
+__global__ void __launch_bounds__(256, 2) k_rns_mma4(RnsMma a, RnsTables tb) {
     extern __shared__ __align__(128) uint8_t smem[];
-    __shared__ __align__(8) uint64_t bar_load[2], bar_mma;
+    __shared__ __align__(8) uint64_t bar_load, bar_mma;
     __shared__ uint32_t tmem_base_sh;
     __shared__ int fail_sh;
 
@@ -320,7 +320,7 @@ __global__ void __launch_bounds__(256, 1) k_rns_mma4(RnsMma a, RnsTables tb) {
     const int64_t g = blockIdx.z, b = blockIdx.y;
     const int64_t ti = blockIdx.x / a.tiles_l, tl = blockIdx.x % a.tiles_l;
     const uint32_t xbytes = 128u * Kp, ybytes = (uint32_t)TN * Kp, stage = xbytes + ybytes;
-    uint8_t* ysm = smem + 2 * (size_t)stage;             // (32 rows i x TN / 4 columns l) x 16 bytes
+    uint8_t* ysm = smem + (size_t)stage;                 // (32 rows i x TN / 4 columns l) x 16 bytes
     const int warp = threadIdx.x / 32;
     const int j0 = (int)g * kPrimesPerCta;
     const int nj = np - j0 < kPrimesPerCta ? np - j0 : kPrimesPerCta;
@@ -329,8 +329,7 @@ __global__ void __launch_bounds__(256, 1) k_rns_mma4(RnsMma a, RnsTables tb) {
 
     if (threadIdx.x == 0) {
         fail_sh = 0;
-        mbar_init(&bar_load[0], 1);
-        mbar_init(&bar_load[1], 1);
+        mbar_init(&bar_load, 1);
         mbar_init(&bar_mma, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -348,9 +347,9 @@ __global__ void __launch_bounds__(256, 1) k_rns_mma4(RnsMma a, RnsTables tb) {
     if (threadIdx.x == 0) {
         const uint8_t* gx = a.X + (size_t)((int64_t)j0 * a.nb + b) * a.x_mat + (size_t)ti * xbytes;
         const uint8_t* gy = a.Y + (size_t)((int64_t)j0 * a.nb + b) * a.y_mat + (size_t)tl * ybytes;
-        mbar_expect_tx(&bar_load[0], stage);
-        bulk_copy_g2s(smem, gx, xbytes, &bar_load[0]);
-        bulk_copy_g2s(smem + xbytes, gy, ybytes, &bar_load[0]);
+        mbar_expect_tx(&bar_load, stage);
+        bulk_copy_g2s(smem, gx, xbytes, &bar_load);
+        bulk_copy_g2s(smem + xbytes, gy, ybytes, &bar_load);
         issued = 1;
     }
     const int row = threadIdx.x & 127, s = row & 3, half = threadIdx.x >> 7;
@@ -360,22 +359,12 @@ __global__ void __launch_bounds__(256, 1) k_rns_mma4(RnsMma a, RnsTables tb) {
 
     for (int pi = 0; pi < nj; pi++) {
         const int j = j0 + pi;
-        const int buf = pi & 1;
-        if (threadIdx.x == 0 && pi + 1 < nj) {           // prefetch prime j + 1 into the other buffer
-            const uint8_t* gx = a.X + (size_t)((int64_t)(j + 1) * a.nb + b) * a.x_mat + (size_t)ti * xbytes;
-            const uint8_t* gy = a.Y + (size_t)((int64_t)(j + 1) * a.nb + b) * a.y_mat + (size_t)tl * ybytes;
-            uint8_t* dst = smem + (size_t)(buf ^ 1) * stage;
-            mbar_expect_tx(&bar_load[buf ^ 1], stage);
-            bulk_copy_g2s(dst, gx, xbytes, &bar_load[buf ^ 1]);
-            bulk_copy_g2s(dst + xbytes, gy, ybytes, &bar_load[buf ^ 1]);
-            issued = pi + 2;
-        }
-        if (!mbar_wait(&bar_load[buf], (pi >> 1) & 1, kWaitLimit)) atomicExch(&fail_sh, 1);
+        if (!mbar_wait(&bar_load, pi & 1, kWaitLimit)) atomicExch(&fail_sh, 1);
         else if (threadIdx.x == 0) waited = pi + 1;
         __syncthreads();
         if (fail_sh) break;
         if (threadIdx.x == 0) {
-            const uint32_t ax = smem_u32(smem + (size_t)buf * stage), ay = ax + xbytes;
+            const uint32_t ax = smem_u32(smem), ay = ax + xbytes;
             for (int kk = 0; kk < Kp / 32; kk++) {
                 uint64_t da = umma_desc(ax + kk * 2 * (128 * 16), 128 * 16, 128);
                 uint64_t db = umma_desc(ay + kk * 2 * (TN * 16), TN * 16, 128);
@@ -395,6 +384,14 @@ __global__ void __launch_bounds__(256, 1) k_rns_mma4(RnsMma a, RnsTables tb) {
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         __syncthreads();
         if (fail_sh) break;
+        if (threadIdx.x == 0 && pi + 1 < nj) {           // the MMAs are done with the buffer: prime j + 1
+            const uint8_t* gx = a.X + (size_t)((int64_t)(j + 1) * a.nb + b) * a.x_mat + (size_t)ti * xbytes;
+            const uint8_t* gy = a.Y + (size_t)((int64_t)(j + 1) * a.nb + b) * a.y_mat + (size_t)tl * ybytes;
+            mbar_expect_tx(&bar_load, stage);
+            bulk_copy_g2s(smem, gx, xbytes, &bar_load);
+            bulk_copy_g2s(smem + xbytes, gy, ybytes, &bar_load);
+            issued = pi + 2;
+        }
 
         const uint32_t p = __ldg(tb.p + j);
         const uint64_t mu = __ldg(tb.mu + j);
@@ -451,7 +448,7 @@ __global__ void __launch_bounds__(256, 1) k_rns_mma4(RnsMma a, RnsTables tb) {
     }
     if (threadIdx.x == 0 && fail_sh) {                    // bounded drain of our own copies and MMAs
         for (int q = waited; q < issued; q++)
-            if (!mbar_wait(&bar_load[q & 1], (q >> 1) & 1, kWaitLimit)) { fail_sh = 3; break; }
+            if (!mbar_wait(&bar_load, q & 1, kWaitLimit)) { fail_sh = 3; break; }
         if (fail_sh != 3 && mma_pending && !mbar_wait(&bar_mma, (waited - 1) & 1, kWaitLimit)) fail_sh = 4;
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");

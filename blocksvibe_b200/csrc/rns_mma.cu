@@ -11,14 +11,14 @@ int rns_mma_launch(const RnsMma& a, const RnsTables& tb, cudaStream_t st) {
         int rc = (int)cudaFuncSetAttribute(k_rns_mma, cudaFuncAttributeMaxDynamicSharedMemorySize, (128 + 256) * 256);
         if (rc) return rc;
         rc = (int)cudaFuncSetAttribute(k_rns_mma4, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       2 * (128 + 256) * 256 + 128 * 256);
+                                       (128 + 256) * 256 + 128 * 256);
         if (rc) return rc;
         configured = true;
     }
     const int64_t tiles_i = (4 * a.NI + 127) / 128;
     const int groups = (tb.np + kPrimesPerCta - 1) / kPrimesPerCta;
     if (a.yb && a.crt_kp >= 16 * groups && a.TN % 16 == 0) {      // CRT operand: four primes per CTA
-        const int smem4 = 2 * (128 + a.TN) * a.Kp + 128 * a.TN;
+        const int smem4 = (128 + a.TN) * a.Kp + 128 * a.TN;
         dim3 grid4((unsigned)(tiles_i * a.tiles_l), (unsigned)a.nb, (unsigned)groups);
         k_rns_mma4<<<grid4, 256, smem4, st>>>(a, tb);
         return (int)cudaGetLastError();
