@@ -364,6 +364,7 @@ __global__ void __launch_bounds__(256, 2) k_rns_mma4(RnsMma a, RnsTables tb) {
         __syncthreads();
         if (fail_sh) break;
         if (threadIdx.x == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");   // after the previous epilogue's reads
             const uint32_t ax = smem_u32(smem), ay = ax + xbytes;
             for (int kk = 0; kk < Kp / 32; kk++) {
                 uint64_t da = umma_desc(ax + kk * 2 * (128 * 16), 128 * 16, 128);
@@ -492,7 +493,7 @@ __global__ void __launch_bounds__(128, 1) k_rns_split_mma(RnsSplit a, RnsTables 
     const int64_t b = blockIdx.y;
     const int64_t ktiles = a.Kp / 16;
     const int64_t r0 = (blockIdx.x / ktiles) * 8, k0 = (blockIdx.x % ktiles) * 16;
-    const uint32_t ncols = 512;
+    const uint32_t ncols = 256;                          // one half (NS <= 256 columns) at a time
     if (t == 0) {
         fail_sh = 0;
         mbar_init(&bar_load, 1);
@@ -540,41 +541,45 @@ __global__ void __launch_bounds__(128, 1) k_rns_split_mma(RnsSplit a, RnsTables 
     if (!mbar_wait(&bar_load, 0, kWaitLimit)) atomicExch(&fail_sh, 1);
     __syncthreads();
     bool run = fail_sh == 0;
-    if (run && t == 0) {
+    int mma_h = 0;                                        // pass of the last MMA commit (failure drain)
+    // two passes over the halves of the constant matrix, sharing 256 TMEM columns (two CTAs per SM)
+    for (int h = 0; h < 2 && run; h++) {
+    if (t == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");   // after the first half's TMEM reads
         const uint32_t idesc = (2u << 4) | ((uint32_t)(NS >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
         const uint32_t aa = smem_u32(sA), ac = smem_u32(sC);
-        for (int h = 0; h < 2; h++) {
-            for (int kk = 0; kk < Ks / 32; kk++) {
-                uint64_t da = umma_desc(aa + kk * 2 * (128 * 16), 128 * 16, 128);
-                uint64_t db = umma_desc(ac + h * NS * Ks + kk * 2 * (NS * 16), NS * 16, 128);
-                uint32_t acc = kk > 0 ? 1u : 0u;
-                asm volatile(
-                    "{\n\t.reg .pred p;\n\t"
-                    "setp.ne.b32 p, %4, 0;\n\t"
-                    "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}"
-                    ::"r"(tmem + (uint32_t)(h * NS)), "l"(da), "l"(db), "r"(idesc), "r"(acc) : "memory");
-            }
+        for (int kk = 0; kk < Ks / 32; kk++) {
+            uint64_t da = umma_desc(aa + kk * 2 * (128 * 16), 128 * 16, 128);
+            uint64_t db = umma_desc(ac + h * NS * Ks + kk * 2 * (NS * 16), NS * 16, 128);
+            uint32_t acc = kk > 0 ? 1u : 0u;
+            asm volatile(
+                "{\n\t.reg .pred p;\n\t"
+                "setp.ne.b32 p, %4, 0;\n\t"
+                "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}"
+                ::"r"(tmem), "l"(da), "l"(db), "r"(idesc), "r"(acc) : "memory");
         }
         asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
                      ::"r"(smem_u32(&bar_mma)) : "memory");
     }
-    if (run && !mbar_wait(&bar_mma, 0, kWaitLimit)) atomicExch(&fail_sh, 2);
+    mma_h = h;
+    if (!mbar_wait(&bar_mma, h, kWaitLimit)) atomicExch(&fail_sh, 2);
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     __syncthreads();
-    run = run && fail_sh == 0;
+    run = fail_sh == 0;
     if (run) {
-        // epilogue: element e = t; residues of 4 primes per 16-column chunk
+        // epilogue: element e = t; residues of 4 primes per 16-column chunk, primes of this half
         const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16);
         const bool neg = neg_sh[t];
         const int rr = t / 16, kk = t % 16;
-        for (int j0 = 0; j0 < np; j0 += 4) {
+        const int jlo = h * (NS / 4), jhi = (h + 1) * (NS / 4) < np ? (h + 1) * (NS / 4) : np;
+        for (int j0 = jlo; j0 < jhi; j0 += 4) {
             uint32_t d[16];
             asm volatile(
                 "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
                 "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
                 : "=r"(d[0]), "=r"(d[1]), "=r"(d[2]), "=r"(d[3]), "=r"(d[4]), "=r"(d[5]), "=r"(d[6]), "=r"(d[7]),
                   "=r"(d[8]), "=r"(d[9]), "=r"(d[10]), "=r"(d[11]), "=r"(d[12]), "=r"(d[13]), "=r"(d[14]), "=r"(d[15])
-                : "r"(taddr + (uint32_t)(4 * j0)));
+                : "r"(taddr + (uint32_t)(4 * j0 - h * NS)));
             asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
             for (int q = 0; q < 4; q++) {
@@ -590,6 +595,10 @@ __global__ void __launch_bounds__(128, 1) k_rns_split_mma(RnsSplit a, RnsTables 
             }
         }
     }
+    mma_h = h;
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();                                      // TMEM read out before the second half's MMAs
+    }
     __syncthreads();
     if (run) {
         // 16-byte chunks: (prime j, digit s, row rr) -> row 4 (r0 + rr) + s, columns k0 .. k0 + 15
@@ -603,7 +612,7 @@ __global__ void __launch_bounds__(128, 1) k_rns_split_mma(RnsSplit a, RnsTables 
     }
     if (t == 0 && fail_sh) {
         if (!mbar_wait(&bar_load, 0, kWaitLimit)) fail_sh = 3;
-        else if (fail_sh == 2 && !mbar_wait(&bar_mma, 0, kWaitLimit)) fail_sh = 4;
+        else if (fail_sh == 2 && !mbar_wait(&bar_mma, mma_h, kWaitLimit)) fail_sh = 4;
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
