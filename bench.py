@@ -55,9 +55,14 @@ def dist_setup():
     if world > 1:
         import datetime
         import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
-                                device_id=torch.device("cuda", local))
+        # replicas only: the process group carries the barrier and the max over ranks of the timings (NCCL on
+        # GPUs; gloo on CPU, as the multi-process tests run it)
+        if torch.cuda.is_available() and os.environ.get("B3D_DIST_BACKEND", "nccl") == "nccl":
+            torch.cuda.set_device(local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                    device_id=torch.device("cuda", local))
+        else:
+            dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=120))
     return world, rank, local
 
 
