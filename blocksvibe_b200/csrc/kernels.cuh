@@ -347,7 +347,10 @@ __global__ void k_cauchy3(const int32_t* __restrict__ xm, const i64* __restrict_
             if (d1 < 0) { n1 = !n1; d1 = -d1; }
             const bool live0 = d0 != 0, live1 = d1 != 0;
             const u32 v0 = live0 ? (u32)d0 : 1u, v1 = live1 ? (u32)d1 : 1u;
-            const u32 i0 = 0xFFFFFFFFu / v0, i1 = 0xFFFFFFFFu / v1;
+            // inv = floor(2^32 / d) (2^32 - 1 for d = 1): for c < 2^32 the estimate umulhi(c, inv) is the
+            // quotient or one below it (c inv / 2^32 > c / d - 1), so one correction step suffices
+            const u32 i0 = v0 == 1u ? 0xFFFFFFFFu : (u32)(0x100000000ull / v0);
+            const u32 i1 = v1 == 1u ? 0xFFFFFFFFu : (u32)(0x100000000ull / v1);
             const int s0 = !live0 ? 0 : (n0 ? -1 : 1), s1 = !live1 ? 0 : (n1 ? -1 : 1);
             u32 r0 = 0, r1 = 0;
 #pragma unroll
@@ -356,15 +359,12 @@ __global__ void k_cauchy3(const int32_t* __restrict__ xm, const i64* __restrict_
                 const int width = j == 0 ? TB - W * (ND - 1) : W;
                 const u32 c0 = (r0 << width) | dividend_bits(a0, lo, width);
                 const u32 c1 = (r1 << width) | dividend_bits(a1, lo, width);
-                u32 q0 = umulhi32(c0, i0), q1 = umulhi32(c1, i1);   // at most 2 short
+                u32 q0 = umulhi32(c0, i0), q1 = umulhi32(c1, i1);   // at most 1 short
                 r0 = c0 - q0 * v0;
                 r1 = c1 - q1 * v1;
                 const bool x0 = r0 >= v0, x1 = r1 >= v1;
                 q0 += x0; r0 -= x0 ? v0 : 0u;
                 q1 += x1; r1 -= x1 ? v1 : 0u;
-                const bool y0 = r0 >= v0, y1 = r1 >= v1;
-                q0 += y0; r0 -= y0 ? v0 : 0u;
-                q1 += y1; r1 -= y1 ? v1 : 0u;
                 acc[j] += s0 * (int)q0 + s1 * (int)q1;
             }
         }
