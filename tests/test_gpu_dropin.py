@@ -51,7 +51,27 @@ def make_group(tj12=2, tj43=2, tjmax=4, order=8, Lam=4, precision=256, kept=5, s
 
 
 def test_dropin_matches_oracle_chain(cuda):
-    G, tasks, M, hstr, plan = make_group()
+    worst = chain_worst_bits(cuda, *make_group())
+    assert worst > 32 * DI.limbs(256) - 40, worst
+
+
+@pytest.mark.parametrize("name,args", [
+    ("cfg1", dict(tj12=0, tj43=0, tjmax=12, order=10, Lam=5, precision=256, kept=6, nq=1, coords=("xt",))),
+    ("cfg1_radial_odd", dict(tj12=0, tj43=0, tjmax=12, order=10, Lam=5, precision=256, kept=6, nq=1,
+                             coords=("xt_radial",), sign=-1)),
+    ("cfg2_shape_512", dict(tj12=8, tj43=8, tjmax=8, order=8, Lam=5, precision=512, kept=5, nq=1, coords=("xt",))),
+    ("cfg2_shape_1024", dict(tj12=8, tj43=8, tjmax=4, order=6, Lam=3, precision=1024, kept=4, nq=1, coords=("xt",))),
+])
+def test_worst_bits_per_config(cuda, name, args):
+    """the north star's bar: every output agrees with the oracle chain to more than prec - 8 bits (relative to
+    each polynomial's largest coefficient); the worst case is printed per configuration"""
+    G, tasks, M, hstr, plan = make_group(**args)
+    worst = chain_worst_bits(cuda, G, tasks, M, hstr, plan)
+    print(f"\nworst-case agreement {name}: {worst:.1f} bits (precision {G.precision}, NB {32 * DI.limbs(G.precision) - 2})")
+    assert worst > G.precision - 8, worst
+
+
+def chain_worst_bits(cuda, G, tasks, M, hstr, plan):
     L = DI.limbs(G.precision)
     res = DI.run_group(G, tasks, M, device=cuda, schedule="plain")
     Sm = plan.Smax
@@ -61,15 +81,15 @@ def test_dropin_matches_oracle_chain(cuda):
     ns = t0.lambda_orders(G.Lambda)
     nums = {n: oracle_numerators(M, hstr[(0, n)], G.two_j12, G.two_j43, G.two_j_max, G.order, t0.pp, L, 0,
                                  G.Lambda - n, tjs, G.kept_pole_order) for n in ns}
-    m, e = vals[("xt", t0.delta_1_plus_2)]
-    got_xt = mpf.to_mp(mpf.MPF(torch.from_numpy(m), torch.from_numpy(e)))      # (Jo, 2, S2, outputs, Dmax)
-    m, e = vals[("xt_radial", t0.delta_1_plus_2)]
-    got_rad = mpf.to_mp(mpf.MPF(torch.from_numpy(m), torch.from_numpy(e)))
+    got = {}
+    for c in t0.coordinates:
+        m, e = vals[(c, t0.delta_1_plus_2)]
+        got[c] = mpf.to_mp(mpf.MPF(torch.from_numpy(m), torch.from_numpy(e)))      # (Jo, 2, S2, outputs, Dmax)
     worst = float("inf")
     with mp.workprec(32 * L + 128):
         for (tj, p, a, b), _ in nums[ns[0]].items():
             jo = tjs.index(tj)
-            Dmax = got_xt.shape[-1]
+            Dmax = next(iter(got.values())).shape[-1]
             for dcoef in range(Dmax):
                 # num[idx][e] for coefficient dcoef
                 table = []
@@ -77,15 +97,17 @@ def test_dropin_matches_oracle_chain(cuda):
                     polys = nums[n][(tj, p, a, b)]
                     table.append([polys[ee][dcoef] if ee <= G.Lambda - n and dcoef < len(polys[ee]) else mp.mpf(0)
                                   for ee in range(G.Lambda - t0.parity + 1)])
-                ref_xt = [x for row in OO.xt(table, G.Lambda, t0.parity, t0.delta_1_plus_2) for x in row]
-                ref_rad = OO.xt_radial(table[0], G.Lambda, t0.parity, t0.delta_1_plus_2)
-                g_xt = [got_xt[jo, p, a * Sm + b, o, dcoef] for o in range(len(ref_xt))]
-                g_rad = [got_rad[jo, p, a * Sm + b, o, dcoef] for o in range(len(ref_rad))]
-                for g, r in ((g_xt, ref_xt), (g_rad, ref_rad)):
+                refs = {}
+                if "xt" in got:
+                    refs["xt"] = [x for row in OO.xt(table, G.Lambda, t0.parity, t0.delta_1_plus_2) for x in row]
+                if "xt_radial" in got:
+                    refs["xt_radial"] = OO.xt_radial(table[0], G.Lambda, t0.parity, t0.delta_1_plus_2)
+                for c, r in refs.items():
                     if max(abs(x) for x in r) == 0:
                         continue
+                    g = [got[c][jo, p, a * Sm + b, o, dcoef] for o in range(len(r))]
                     worst = min(worst, agreement_bits(g, r))
-    assert worst > 32 * L - 40, worst
+    return float(worst)
 
 
 def test_batched_schedule_is_bitwise_plain(cuda):
