@@ -419,10 +419,14 @@ __global__ void k_cauchy3(const int32_t* __restrict__ xm, const i64* __restrict_
 }
 
 // ------------------------------------------------------------------------------------------------
+// The pole kernels keep their 2 L + 2 accumulator limbs in shared memory (one column per thread), so that only
+// the operands live in registers: more resident warps to hide the latency of the multiply-add chains.
+constexpr int kPoleThreads = 128;
+
 // Pole step, stage 1: Y[t, a, b0, k] = sum_b R[b0, b] H[t_hrow[t], a, b, k]  (R = Rtab[t_R[t]] aligned
 // per row; H aligned per column (a, k) over b here).  Y: (T, S, S, B) contiguous.
 template <int L>
-__global__ void k_pole1(const int32_t* __restrict__ hm, const i64* __restrict__ he, i64 hplane,
+__global__ void __launch_bounds__(kPoleThreads, 3) k_pole1(const int32_t* __restrict__ hm, const i64* __restrict__ he, i64 hplane,
                         const int32_t* __restrict__ Rm, const i64* __restrict__ Re, i64 Rplane,
                         const i64* __restrict__ t_hrow, const i64* __restrict__ t_R, i64 T, i64 B, int S,
                         int32_t* __restrict__ ym, i64* __restrict__ ye, i64 yplane) {
@@ -439,8 +443,10 @@ __global__ void k_pole1(const int32_t* __restrict__ hm, const i64* __restrict__ 
     }
     i64 Er = Re[rk * S + b0];
     constexpr int NW = 2 * L + 2;
-    u32 acc[NW];
-    zero(acc);
+    extern __shared__ u32 pole_acc[];                    // (NW, blockDim.x): this thread's column
+    u32* acc = pole_acc + threadIdx.x;
+#pragma unroll
+    for (int w = 0; w < NW; w++) acc[w * kPoleThreads] = 0;
     if (E != EZ && Er != EZ) {
 #pragma unroll 1
         for (int b = 0; b < S; b++) {
@@ -452,16 +458,19 @@ __global__ void k_pole1(const int32_t* __restrict__ hm, const i64* __restrict__ 
             i64 ex = he[ix];
             if (is_zero(x) || ex == EZ || E - ex >= 32 * L) continue;
             shr(x, (int)(E - ex), y);
-            mac_signed<L, NW>(acc, r, y, nr != nx);
+            mac_signed_mem<L, NW>(acc, kPoleThreads, r, y, nr != nx);
         }
     }
-    store_rounded<L, NW>(ym, ye, yplane, idx, acc, (E == EZ || Er == EZ) ? EZ : E + Er);
+    u32 accr[NW];
+#pragma unroll
+    for (int w = 0; w < NW; w++) accr[w] = acc[w * kPoleThreads];
+    store_rounded<L, NW>(ym, ye, yplane, idx, accr, (E == EZ || Er == EZ) ? EZ : E + Er);
 }
 
 // Pole step, stage 2: res[t_slot[t], a0, b0, k] = sum_a QL[a0, a] Y[t, a, b0, k]  (QL = QLtab[t_qL[t]]
 // aligned per row; Y aligned per column (b0, k) over a here).
 template <int L>
-__global__ void k_pole2(const int32_t* __restrict__ ym, const i64* __restrict__ ye, i64 yplane,
+__global__ void __launch_bounds__(kPoleThreads, 3) k_pole2(const int32_t* __restrict__ ym, const i64* __restrict__ ye, i64 yplane,
                         const int32_t* __restrict__ Qm, const i64* __restrict__ Qe, i64 Qplane,
                         const i64* __restrict__ t_qL, const i64* __restrict__ t_slot, i64 T, i64 B, int S,
                         int32_t* __restrict__ rm, i64* __restrict__ re, i64 rplane) {
@@ -478,8 +487,10 @@ __global__ void k_pole2(const int32_t* __restrict__ ym, const i64* __restrict__ 
     }
     i64 Eq = Qe[qk * S + a0];
     constexpr int NW = 2 * L + 2;
-    u32 acc[NW];
-    zero(acc);
+    extern __shared__ u32 pole_acc[];                    // (NW, blockDim.x): this thread's column
+    u32* acc = pole_acc + threadIdx.x;
+#pragma unroll
+    for (int w = 0; w < NW; w++) acc[w * kPoleThreads] = 0;
     if (E != EZ && Eq != EZ) {
 #pragma unroll 1
         for (int a = 0; a < S; a++) {
@@ -491,11 +502,14 @@ __global__ void k_pole2(const int32_t* __restrict__ ym, const i64* __restrict__ 
             i64 ex = ye[ix];
             if (is_zero(x) || ex == EZ || E - ex >= 32 * L) continue;
             shr(x, (int)(E - ex), y);
-            mac_signed<L, NW>(acc, q, y, nq != nx);
+            mac_signed_mem<L, NW>(acc, kPoleThreads, q, y, nq != nx);
         }
     }
+    u32 accr[NW];
+#pragma unroll
+    for (int w = 0; w < NW; w++) accr[w] = acc[w * kPoleThreads];
     i64 out = t_slot[t] * S * S * B + (a0 * S + b0) * B + k;
-    store_rounded<L, NW>(rm, re, rplane, out, acc, (E == EZ || Eq == EZ) ? EZ : E + Eq);
+    store_rounded<L, NW>(rm, re, rplane, out, accr, (E == EZ || Eq == EZ) ? EZ : E + Eq);
 }
 
 // ------------------------------------------------------------------------------------------------
@@ -660,8 +674,11 @@ int Launch<L>::pole(const int32_t* hm, const i64* he, i64 hplane, const int32_t*
                     int32_t* rm, i64* re, i64 rplane, cudaStream_t st) {
     i64 n = T * S * S * B;
     if (n == 0) return 0;
-    k_pole1<L><<<grid_for(n, kThreads), kThreads, 0, st>>>(hm, he, hplane, Rm, Re, Rplane, t_hrow, t_R, T, B, S, ym, ye, yplane);
-    k_pole2<L><<<grid_for(n, kThreads), kThreads, 0, st>>>(ym, ye, yplane, Qm, Qe, Qplane, t_qL, t_slot, T, B, S, rm, re, rplane);
+    const int smem = (2 * L + 2) * kPoleThreads * 4;   // <= 44 KB (L = 42): no opt-in
+    k_pole1<L><<<grid_for(n, kPoleThreads), kPoleThreads, smem, st>>>(hm, he, hplane, Rm, Re, Rplane, t_hrow, t_R, T, B, S,
+                                                                       ym, ye, yplane);
+    k_pole2<L><<<grid_for(n, kPoleThreads), kPoleThreads, smem, st>>>(ym, ye, yplane, Qm, Qe, Qplane, t_qL, t_slot, T, B,
+                                                                       S, rm, re, rplane);
     return (int)cudaGetLastError();
 }
 

@@ -225,6 +225,32 @@ template <int L, int NW> B3D_HD void mac_signed(u32 (&acc)[NW], const u32 (&a)[L
     }
 }
 
+// mac_signed with the accumulator in memory (limb k at acc[k * stride]; shared memory in the pole kernels, so
+// that the operands, not the 2 L + 2 accumulator limbs, occupy the registers): same result bit for bit
+template <int L, int NW> B3D_HD void mac_signed_mem(u32* acc, int stride, const u32 (&a)[L], const u32 (&b)[L],
+                                                    bool negative) {
+    u32 c0 = 0, c1 = 0, c2 = 0;
+    i64 rc = 0;
+#pragma unroll
+    for (int col = 0; col < 2 * L; col++) {
+#pragma unroll
+        for (int x = 0; x < L; x++) {
+            int y = col - x;
+            if (y >= 0 && y < L) mac96(c0, c1, c2, a[x], b[y]);
+        }
+        i64 r = (i64)acc[col * stride] + (negative ? -(i64)c0 : (i64)c0) + rc;
+        acc[col * stride] = (u32)r;
+        rc = r >> 32;
+        c0 = c1; c1 = c2; c2 = 0;
+    }
+#pragma unroll
+    for (int k = 2 * L; k < NW; k++) {
+        i64 r = (i64)acc[k * stride] + rc;
+        acc[k * stride] = (u32)r;
+        rc = r >> 32;
+    }
+}
+
 // acc (two's complement) += sgn * q, q an unsigned magnitude of NQ limbs (NQ <= NW)
 template <int NQ, int NW> B3D_HD void add_signed(u32 (&acc)[NW], const u32 (&q)[NQ], bool negative) {
     i64 rc = 0;
