@@ -310,8 +310,10 @@ __device__ __forceinline__ u32 dividend_bits(const u32 (&a)[L], int lo, int widt
     return width >= 32 ? v : (v & ((1u << width) - 1u));
 }
 
+constexpr int kCauchyThreads = 128;
+
 template <int L, int W>
-__global__ void k_cauchy3(const int32_t* __restrict__ xm, const i64* __restrict__ xe, i64 xplane,
+__global__ void __launch_bounds__(kCauchyThreads, 3) k_cauchy3(const int32_t* __restrict__ xm, const i64* __restrict__ xe, i64 xplane,
                           const int32_t* __restrict__ hm, const i64* __restrict__ he, i64 hplane,
                           CauchyLevel lv, int32_t* __restrict__ om, i64* __restrict__ oe, i64 oplane) {
     constexpr int TB = 32 * (L + 1), ND = (TB + W - 1) / W;
@@ -331,9 +333,10 @@ __global__ void k_cauchy3(const int32_t* __restrict__ xm, const i64* __restrict_
     const i64 ncol = lv.ncol[g];
     const i64* cold = lv.cold + g * lv.Kc;
     const i64 D = lv.rowd[g * lv.Mr + r];
-    int acc[ND];
+    extern __shared__ int c3_acc[];                      // (ND, blockDim.x): this thread's digit sums
+    int* acc = c3_acc + threadIdx.x;
 #pragma unroll
-    for (int j = 0; j < ND; j++) acc[j] = 0;
+    for (int j = 0; j < ND; j++) acc[j * kCauchyThreads] = 0;
     if (E != EZ) {
         for (i64 i = 0; i < ncol; i += 2) {
             u32 a0[L], a1[L];
@@ -365,7 +368,7 @@ __global__ void k_cauchy3(const int32_t* __restrict__ xm, const i64* __restrict_
                 const bool x0 = r0 >= v0, x1 = r1 >= v1;
                 q0 += x0; r0 -= x0 ? v0 : 0u;
                 q1 += x1; r1 -= x1 ? v1 : 0u;
-                acc[j] += s0 * (int)q0 + s1 * (int)q1;
+                acc[j * kCauchyThreads] += s0 * (int)q0 + s1 * (int)q1;
             }
         }
     }
@@ -378,7 +381,7 @@ __global__ void k_cauchy3(const int32_t* __restrict__ xm, const i64* __restrict_
 #pragma unroll
         for (int j = ND - 1; j >= 0; j--) {
             const int lo = W * (ND - 1 - j), k0 = lo >> 5, b0 = lo & 31;
-            const long long v = (long long)acc[j] + carry;
+            const long long v = (long long)acc[j * kCauchyThreads] + carry;
             long long part;
             if (j > 0) {                                    // keep W bits here, carry the rest up
                 part = v & ((1ll << W) - 1);
@@ -658,10 +661,13 @@ int Launch<L>::cauchy3(const int32_t* xm, const i64* xe, i64 xplane, const int32
                        const CauchyLevel& lv, i64 dmax, int32_t* om, i64* oe, i64 oplane, cudaStream_t st) {
     i64 n = lv.nb * lv.Mr * lv.N;
     if (n == 0) return 0;
+    constexpr int TB = 32 * (L + 1);
     if (dmax < (1 << 8) && lv.Kc < 128)
-        k_cauchy3<L, 24><<<grid_for(n, kThreads), kThreads, 0, st>>>(xm, xe, xplane, hm, he, hplane, lv, om, oe, oplane);
+        k_cauchy3<L, 24><<<grid_for(n, kCauchyThreads), kCauchyThreads, ((TB + 23) / 24) * kCauchyThreads * 4, st>>>(
+            xm, xe, xplane, hm, he, hplane, lv, om, oe, oplane);
     else if (dmax < (1 << 10) && lv.Kc < 512)
-        k_cauchy3<L, 22><<<grid_for(n, kThreads), kThreads, 0, st>>>(xm, xe, xplane, hm, he, hplane, lv, om, oe, oplane);
+        k_cauchy3<L, 22><<<grid_for(n, kCauchyThreads), kCauchyThreads, ((TB + 21) / 22) * kCauchyThreads * 4, st>>>(
+            xm, xe, xplane, hm, he, hplane, lv, om, oe, oplane);
     else
         k_cauchy2<L><<<grid_for(n, kThreads), kThreads, 0, st>>>(xm, xe, xplane, hm, he, hplane, lv, om, oe, oplane);
     return (int)cudaGetLastError();
