@@ -520,8 +520,10 @@ __global__ void __launch_bounds__(kPoleThreads, 3) k_pole2(const int32_t* __rest
 //   y = res[slot, c] * rc^n,   mom[row, kk, c] += n^kk y   (kk <= R)
 // mom layout (rows, R + 1, N).  n^kk y is formed exactly from the previous power (one-limb product)
 // and rounded before each addition.
+constexpr int kMomThreads = 128;
+
 template <int L>
-__global__ void k_moments(const int32_t* __restrict__ rm, const i64* __restrict__ re, i64 rplane,
+__global__ void __launch_bounds__(kMomThreads, 3) k_moments(const int32_t* __restrict__ rm, const i64* __restrict__ re, i64 rplane,
                           const int32_t* __restrict__ pm, const i64* __restrict__ pe, i64 pplane,
                           const i64* __restrict__ q_slot, const i64* __restrict__ q_row, const i64* __restrict__ q_n,
                           i64 Q, i64 N, int R1, int32_t* __restrict__ mm, i64* __restrict__ me, i64 mplane) {
@@ -535,9 +537,14 @@ __global__ void k_moments(const int32_t* __restrict__ rm, const i64* __restrict_
     i64 ex = re[ix], ep = pe[nn];
     if (is_zero(x) || is_zero(p) || ex == EZ || ep == EZ) return;
     constexpr int NW = 2 * L + 1;
+    extern __shared__ u32 mom_acc[];                     // (NW, blockDim.x): this thread's product
+    u32* accm = mom_acc + threadIdx.x;
+#pragma unroll
+    for (int w = 0; w < NW; w++) accm[w * kMomThreads] = 0;
+    mac_signed_mem<L, NW>(accm, kMomThreads, x, p, false);
     u32 acc[NW];
-    zero(acc);
-    mac_signed<L, NW>(acc, x, p, false);
+#pragma unroll
+    for (int w = 0; w < NW; w++) acc[w] = accm[w * kMomThreads];
     u32 y[L];
     i64 ey;
     round_mag<L>(acc, ex + ep, y, &ey);
@@ -694,7 +701,8 @@ int Launch<L>::moments(const int32_t* rm, const i64* re, i64 rplane, const int32
                        int32_t* mm, i64* me, i64 mplane, cudaStream_t st) {
     i64 n = Q * N;
     if (n == 0) return 0;
-    k_moments<L><<<grid_for(n, kThreads), kThreads, 0, st>>>(rm, re, rplane, pm, pe, pplane, q_slot, q_row, q_n, Q, N, R1, mm, me, mplane);
+    k_moments<L><<<grid_for(n, kMomThreads), kMomThreads, (2 * L + 1) * kMomThreads * 4, st>>>(
+        rm, re, rplane, pm, pe, pplane, q_slot, q_row, q_n, Q, N, R1, mm, me, mplane);
     return (int)cudaGetLastError();
 }
 #endif
