@@ -58,8 +58,10 @@ __global__ void k_align(const int32_t* __restrict__ m, const i64* __restrict__ e
 
 // Batched product of aligned operands: C[b, i, j] = sum_k A[b, i, k] B[b, k, j] with A rows and B
 // columns already aligned (k_align); exact accumulation, one rounding.  C is contiguous (b, i, j).
+constexpr int kGemmThreads = 128;
+
 template <int L>
-__global__ void k_gemm_aligned(const int32_t* __restrict__ am, const i64* __restrict__ ae, i64 aplane,
+__global__ void __launch_bounds__(kGemmThreads, 3) k_gemm_aligned(const int32_t* __restrict__ am, const i64* __restrict__ ae, i64 aplane,
                                const int32_t* __restrict__ bm, const i64* __restrict__ be, i64 bplane,
                                i64 nbatch, i64 M, i64 N, i64 K, int32_t* __restrict__ cm, i64* __restrict__ ce,
                                i64 cplane) {
@@ -68,8 +70,10 @@ __global__ void k_gemm_aligned(const int32_t* __restrict__ am, const i64* __rest
     i64 j = t % N, i = (t / N) % M, b = t / (M * N);
     i64 Ea = ae[b * M + i], Eb = be[b * N + j];
     constexpr int NW = 2 * L + 2;
-    u32 acc[NW];
-    zero(acc);
+    extern __shared__ u32 gemm_acc[];                    // (NW, blockDim.x): this thread's accumulator
+    u32* accm = gemm_acc + threadIdx.x;
+#pragma unroll
+    for (int w = 0; w < NW; w++) accm[w * kGemmThreads] = 0;
     if (Ea != EZ && Eb != EZ) {
         for (i64 k = 0; k < K; k++) {
             u32 a[L], bb[L];
@@ -77,9 +81,12 @@ __global__ void k_gemm_aligned(const int32_t* __restrict__ am, const i64* __rest
             if (is_zero(a)) continue;
             bool nb = load_mag<L>(bm, bplane, (b * K + k) * N + j, bb);
             if (is_zero(bb)) continue;
-            mac_signed<L, NW>(acc, a, bb, na != nb);
+            mac_signed_mem<L, NW>(accm, kGemmThreads, a, bb, na != nb);
         }
     }
+    u32 acc[NW];
+#pragma unroll
+    for (int w = 0; w < NW; w++) acc[w] = accm[w * kGemmThreads];
     store_rounded<L, NW>(cm, ce, cplane, t, acc, (Ea == EZ || Eb == EZ) ? EZ : Ea + Eb);
 }
 
@@ -625,7 +632,8 @@ int Launch<L>::gemm_aligned(const int32_t* am, const i64* ae, i64 aplane, const 
                             i64 nbatch, i64 M, i64 N, i64 K, int32_t* cm, i64* ce, i64 cplane, cudaStream_t st) {
     i64 n = nbatch * M * N;
     if (n == 0) return 0;
-    k_gemm_aligned<L><<<grid_for(n, kThreads), kThreads, 0, st>>>(am, ae, aplane, bm, be, bplane, nbatch, M, N, K, cm, ce, cplane);
+    k_gemm_aligned<L><<<grid_for(n, kGemmThreads), kGemmThreads, (2 * L + 2) * kGemmThreads * 4, st>>>(
+        am, ae, aplane, bm, be, bplane, nbatch, M, N, K, cm, ce, cplane);
     return (int)cudaGetLastError();
 }
 
