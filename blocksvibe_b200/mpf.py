@@ -254,21 +254,19 @@ def gemm_aligned(Aal, Bal):
     return MPF(cm.reshape(L, nb, M, N), ce)
 
 
-# GEMM backend: "auto" (tensor-core RNS GEMM for 8 <= K <= 256, the CUDA-core schoolbook GEMM otherwise),
-# "rns" or "schoolbook" (both give the same bits: exact dot products, one rounding)
+# GEMM backend: "auto" (tensor-core RNS GEMM for RNS_MIN_K <= K <= 256, the CUDA-core schoolbook GEMM otherwise),
+# "rns" or "schoolbook" (both give the same bits: exact dot products, one rounding).  The threshold is measured:
+# at K = 16..31 the residue GEMM is as fast as or faster than the schoolbook one on the derivative and output
+# GEMMs of the bench configurations, at K = 8 it is slower.
 GEMM_BACKEND = "auto"
-RNS_MIN_K = 32
-
-
-RNS_MIN_K_WIDE, RNS_WIDE = 16, 4096
+RNS_MIN_K = 16
 
 
 def _use_rns(K, M=0, N=0):
-    """the residue GEMM pays for its digit split and CRT when K is large, or when K is moderate and one side
-    of the (per batch) product is wide enough to fill the tensor-core tiles"""
+    """the residue GEMM pays for its digit split and CRT once K is large enough"""
     if GEMM_BACKEND == "schoolbook" or K > 256:
         return False
-    return GEMM_BACKEND == "rns" or K >= RNS_MIN_K or (K >= RNS_MIN_K_WIDE and max(M, N) >= RNS_WIDE)
+    return GEMM_BACKEND == "rns" or K >= RNS_MIN_K
 
 
 def gemm(A, B, aidx=None, cache=None, key=None):
