@@ -32,6 +32,8 @@ class Recursion:
         (the level's Cauchy GEMM on the tensor cores, residues + CRT), or "auto" (rns for levels with at least
         rns_min_k columns, cuda2 below)"""
         self.cauchy, self.rns_min_k = cauchy, rns_min_k
+        self._side = {}                                  # calling stream -> stream of the per-level hook
+        self.overlap_hook = True
         if not _lib.lib().b3d_supported_limbs(L):
             raise _lib.B3DError(f"no kernels compiled for L = {L}")
         if plan.dmax >= 1 << 16:
@@ -150,9 +152,11 @@ class Recursion:
         per = (4 * self.L + 8) * self.plan.Smax ** 2 * B
         return per * (self.plan.nphys + 1 + self.max_rows + self.max_tasks)
 
-    def run(self, h_inf, hook=None):
+    def run(self, h_inf, hook=None, overlap=None):
         """h_inf: MPF (2, >= order, Jh, Smax^2, B).  Returns the residue slots MPF (nphys + 1, Smax^2, B);
-        hook(m, res) runs after each level (e.g. Derivs.accumulate)."""
+        hook(m, res) runs after each level (e.g. Derivs.accumulate).  overlap: the hook of level m runs on a
+        second stream, concurrently with the Cauchy step of level m + 1 (which only reads the slots and writes
+        H); the pole step of level m + 1, which writes slots, waits for it.  None: self.overlap_hook."""
         plan, L, Sm = self.plan, self.L, self.plan.Smax
         S2, B = Sm * Sm, h_inf.shape[-1]
         N = S2 * B
@@ -165,7 +169,16 @@ class Recursion:
         res = mpf.zeros((plan.nphys + 1, S2, B), L, dev)
         H = mpf.zeros((max(1, self.max_rows), N), L, dev)
         Y = mpf.zeros((max(1, self.max_tasks), S2, B), L, dev)
-        stream = torch.cuda.current_stream(dev).cuda_stream
+        main = torch.cuda.current_stream(dev)
+        stream = main.cuda_stream
+        side = None
+        if overlap is None:
+            overlap = self.overlap_hook
+        if hook is not None and overlap:
+            side = self._side.get(stream)
+            if side is None:
+                side = self._side[stream] = torch.cuda.Stream(dev)
+        pending = None                                   # the side stream's last hook, not yet joined
         p = lambda t: t.data_ptr()
         for lev in self.levels:
             if lev is None:
@@ -190,13 +203,26 @@ class Recursion:
             else:
                 _lib.call("b3d_cauchy_level", L, p(res.m), p(res.e), res.m.stride(0), p(h_inf.m), p(h_inf.e),
                           h_inf.m.stride(0), _lib.ctypes_byref(tabs), p(H.m), p(H.e), H.m.stride(0), stream)
+            if pending is not None:                      # slots written below may still be read by the hook
+                main.wait_event(pending)
+                pending = None
             _lib.call("b3d_pole_level", L, p(H.m), p(H.e), H.m.stride(0),
                       p(self.Ralign[0]), p(self.Ralign[1]), self.Ralign[0].stride(0),
                       p(self.QLalign[0]), p(self.QLalign[1]), self.QLalign[0].stride(0),
                       p(lev["t_hrow"]), p(lev["t_R"]), p(lev["t_qL"]), p(lev["t_slot"]), lev["T"], B, Sm,
                       p(Y.m), p(Y.e), Y.m.stride(0), p(res.m), p(res.e), res.m.stride(0), stream)
-            if hook is not None:
+            if hook is not None and side is not None:
+                ready = torch.cuda.Event()
+                ready.record(main)
+                side.wait_event(ready)
+                with torch.cuda.stream(side):
+                    hook(lev["m"], res)
+                pending = torch.cuda.Event()
+                pending.record(side)
+            elif hook is not None:
                 hook(lev["m"], res)
+        if pending is not None:
+            main.wait_event(pending)
         return res
 
     def slot(self, p, m, jidx, pidx):
