@@ -191,9 +191,10 @@ def _split(tb, m, plane, nb, R, K, sb, sr, sk, Kp, TR, stream):
     return out, mat, Rp
 
 
-def gemm_aligned_rns(Aal, Bal, crt="tensor"):
+def gemm_aligned_rns(Aal, Bal, crt="tensor", lanes=None):
     """(row-aligned A (L, nb, M, K), (nb, M)) x (column-aligned B (L, nb, K, N), (nb, N)) -> MPF (nb, M, N),
-    on the tensor cores; K <= 256"""
+    on the tensor cores; K <= 256.  lanes: "a" or "b", the operand whose rows go on the 128 TMEM lanes
+    (default: the one with more rows)"""
     am, ae = Aal
     bm, be = Bal
     L, nb, M, K = am.shape
@@ -207,7 +208,7 @@ def gemm_aligned_rns(Aal, Bal, crt="tensor"):
     # the operand with more rows goes on the 128 TMEM lanes
     a_rows = dict(m=am, plane=am.stride(0), R=M, sb=M * K, sr=K, sk=1)
     b_rows = dict(m=bm, plane=bm.stride(0), R=N, sb=K * N, sr=1, sk=N)
-    if M >= N:
+    if (lanes is None and M >= N) or lanes == "a":
         xs, ys, out_i, out_l = a_rows, b_rows, N, 1
     else:
         xs, ys, out_i, out_l = b_rows, a_rows, 1, N

@@ -50,3 +50,38 @@ def test_rns_gemm_cancellation(cuda):
     for crt in ("tensor", "cuda"):
         got = rns.gemm_aligned_rns(Aal, Bal, crt=crt)
         assert torch.equal(ref.m, got.m) and torch.equal(ref.e, got.e)
+
+
+@pytest.mark.parametrize("lanes", ["a", "b"])
+@pytest.mark.parametrize("L,nb,M,K,N", [(10, 2, 40, 33, 70), (34, 1, 66, 98, 300), (42, 3, 28, 28, 50)])
+def test_rns_gemm_either_operand_on_the_lanes(cuda, lanes, L, nb, M, K, N):
+    rns.SPLIT = "tensor"
+    g = torch.Generator().manual_seed(L + M + K + N)
+    A = mpf.random_mpf((nb, M, K), L, spread=20, device=cuda, generator=g)
+    B = mpf.random_mpf((nb, K, N), L, spread=20, device=cuda, generator=g)
+    Aal, Bal = mpf.align_rows(A), mpf.align_cols(B)
+    ref = mpf.gemm_aligned(Aal, Bal)
+    got = rns.gemm_aligned_rns(Aal, Bal, lanes=lanes)
+    rns.check_errors(cuda)
+    assert torch.equal(ref.m, got.m) and torch.equal(ref.e, got.e)
+
+
+def test_autotuned_gemm_equals_schoolbook(cuda):
+    """the autotuner times the candidate paths per shape and keeps the fastest; every path gives the same bits"""
+    rns.SPLIT = "tensor"
+    g = torch.Generator().manual_seed(77)
+    shapes = [(34, 1, 21, 21, 3000), (34, 40, 12, 12, 50), (18, 2, 66, 98, 200)]
+    try:
+        for L, nb, M, K, N in shapes:
+            A = mpf.random_mpf((nb, M, K), L, spread=10, device=cuda, generator=g)
+            B = mpf.random_mpf((nb, K, N), L, spread=10, device=cuda, generator=g)
+            mpf.GEMM_BACKEND, mpf.AUTOTUNE = "schoolbook", True
+            ref = mpf.gemm(A, B)
+            mpf.GEMM_BACKEND = "auto"
+            first = mpf.gemm(A, B)                     # tunes this shape
+            again = mpf.gemm(A, B)                     # uses the choice
+            assert (L, nb, M, N, K, cuda.index or 0) in mpf.tuned_paths()
+            for got in (first, again):
+                assert torch.equal(ref.m, got.m) and torch.equal(ref.e, got.e)
+    finally:
+        mpf.GEMM_BACKEND, mpf.AUTOTUNE = "auto", False
