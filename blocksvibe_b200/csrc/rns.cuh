@@ -490,9 +490,7 @@ __global__ void __launch_bounds__(128, 1) k_rns_split_mma(RnsSplit a, RnsTables 
     uint8_t* sC = smem + 128 * Ks;                       // 2 NS x Ks constants
     uint8_t* sD = sC + 2 * NS * Ks;                      // np x 4 x 8 x 16 staged digits
     const int warp = threadIdx.x / 32, t = threadIdx.x;
-    const int64_t b = blockIdx.y;
-    const int64_t ktiles = a.Kp / 16;
-    const int64_t r0 = (blockIdx.x / ktiles) * 8, k0 = (blockIdx.x % ktiles) * 16;
+    const int64_t ktiles = a.Kp / 16, tiles = ktiles * ((a.Rp + 7) / 8), items = tiles * a.nb;
     const uint32_t ncols = 256;                          // one half (NS <= 256 columns) at a time
     if (t == 0) {
         fail_sh = 0;
@@ -514,6 +512,14 @@ __global__ void __launch_bounds__(128, 1) k_rns_split_mma(RnsSplit a, RnsTables 
         mbar_expect_tx(&bar_load, cbytes);
         bulk_copy_g2s(sC, a.C, cbytes, &bar_load);
     }
+    if (!mbar_wait(&bar_load, 0, kWaitLimit)) atomicExch(&fail_sh, 1);
+    __syncthreads();
+    bool run = fail_sh == 0;
+    int mma_h = 0;                                        // pass of the last MMA commit (failure drain)
+    // persistent: the constant and the TMEM allocation serve every tile this CTA takes
+    for (int64_t item = blockIdx.x; item < items && run; item += gridDim.x) {
+    const int64_t b = item / tiles, tile = item % tiles;
+    const int64_t r0 = (tile / ktiles) * 8, k0 = (tile % ktiles) * 16;
     // magnitudes of the tile's elements -> A rows e = rr * 16 + kk (load order follows the unit stride)
     {
         const bool rows_fast = a.sr == 1;
@@ -538,10 +544,7 @@ __global__ void __launch_bounds__(128, 1) k_rns_split_mma(RnsSplit a, RnsTables 
             *reinterpret_cast<uint4*>(sA + tiled_offset(e, 16 * c, 128, Ks)) = make_uint4(0, 0, 0, 0);
     }
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");    // generic-proxy writes -> tensor core
-    if (!mbar_wait(&bar_load, 0, kWaitLimit)) atomicExch(&fail_sh, 1);
     __syncthreads();
-    bool run = fail_sh == 0;
-    int mma_h = 0;                                        // pass of the last MMA commit (failure drain)
     // two passes over the halves of the constant matrix, sharing 256 TMEM columns (two CTAs per SM)
     for (int h = 0; h < 2 && run; h++) {
     if (t == 0) {
@@ -609,6 +612,8 @@ __global__ void __launch_bounds__(128, 1) k_rns_split_mma(RnsSplit a, RnsTables 
             uint4 w = *reinterpret_cast<const uint4*>(sD + (size_t)c * 16);
             *reinterpret_cast<uint4*>(a.out + ((size_t)j * a.nb + b) * a.mat_bytes + tiled_offset(4 * r + s, k0, a.TR, a.Kp)) = w;
         }
+    }
+    __syncthreads();                                      // sD and neg_sh are rewritten by the next tile
     }
     if (t == 0 && fail_sh) {
         if (!mbar_wait(&bar_load, 0, kWaitLimit)) fail_sh = 3;
@@ -873,8 +878,16 @@ int RnsLaunch<L>::split_mma(const RnsSplit& a, const RnsTables& tb, cudaStream_t
         configured = true;
     }
     if (a.nb == 0 || a.Rp == 0) return 0;
-    dim3 grid((unsigned)((a.Kp / 16) * ((a.Rp + 7) / 8)), (unsigned)a.nb);
-    k_rns_split_mma<L><<<grid, 128, smem, st>>>(a, tb);
+    static int sms = 0;
+    if (!sms) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (sms <= 0) sms = 148;
+    }
+    const int64_t items = (a.Kp / 16) * ((a.Rp + 7) / 8) * a.nb;
+    const int64_t ctas = items < 2 * (int64_t)sms ? items : 2 * (int64_t)sms;   // two CTAs per SM, persistent
+    k_rns_split_mma<L><<<(unsigned)ctas, 128, smem, st>>>(a, tb);
     return (int)cudaGetLastError();
 }
 
