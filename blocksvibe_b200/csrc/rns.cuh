@@ -678,15 +678,26 @@ __global__ void __launch_bounds__(128, 1) k_rns_crt_mma(RnsCrt a, RnsTables tb) 
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = tmem_base_sh;
-    if (threadIdx.x == 0) {
+    // persistent over tiles of 128 outputs: the constant T is loaded once; the next tile's y bytes are copied
+    // into sA as soon as the MMAs of the current tile have completed, while its epilogue runs
+    const int64_t tiles = (a.n + 127) / 128;
+    int issued = 0, waited = 0, mma_pending = 0;          // thread 0's bookkeeping (failure drain)
+    if (threadIdx.x == 0 && (int64_t)blockIdx.x < tiles) {
         mbar_expect_tx(&bar_load, abytes + tbytes);
         bulk_copy_g2s(sA, a.A + (size_t)blockIdx.x * abytes, abytes, &bar_load);
         bulk_copy_g2s(sT, a.T, tbytes, &bar_load);
+        issued = 1;
     }
-    if (!mbar_wait(&bar_load, 0, kWaitLimit)) atomicExch(&fail_sh, 1);
+    bool run = true;
+    int it = 0;
+    for (int64_t tile = blockIdx.x; tile < tiles && run; tile += gridDim.x, it++) {
+    if (!mbar_wait(&bar_load, it & 1, kWaitLimit)) atomicExch(&fail_sh, 1);
+    else if (threadIdx.x == 0) waited = it + 1;
     __syncthreads();
-    bool run = fail_sh == 0;
-    if (run && threadIdx.x == 0) {
+    run = fail_sh == 0;
+    if (!run) break;
+    if (threadIdx.x == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");   // after the previous epilogue's reads
         const uint32_t idesc = (2u << 4) | ((uint32_t)(NH >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
         const uint32_t aa = smem_u32(sA), at = smem_u32(sT);
         for (int h = 0; h < 2; h++) {
@@ -703,13 +714,21 @@ __global__ void __launch_bounds__(128, 1) k_rns_crt_mma(RnsCrt a, RnsTables tb) 
         }
         asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
                      ::"r"(smem_u32(&bar_mma)) : "memory");
+        mma_pending = 1;
     }
-    if (run && !mbar_wait(&bar_mma, 0, kWaitLimit)) atomicExch(&fail_sh, 2);
+    if (!mbar_wait(&bar_mma, it & 1, kWaitLimit)) atomicExch(&fail_sh, 2);
+    else if (threadIdx.x == 0) mma_pending = 0;
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     __syncthreads();
-    run = run && fail_sh == 0;
-    const int64_t e = (int64_t)blockIdx.x * 128 + threadIdx.x;
-    if (run) {
+    run = fail_sh == 0;
+    if (!run) break;
+    if (threadIdx.x == 0 && tile + gridDim.x < tiles) {  // the MMAs are done with sA: the next tile
+        mbar_expect_tx(&bar_load, abytes);
+        bulk_copy_g2s(sA, a.A + (size_t)(tile + gridDim.x) * abytes, abytes, &bar_load);
+        issued = it + 2;
+    }
+    const int64_t e = tile * 128 + threadIdx.x;
+    {
         const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16);
         u32 x[NX];
         uint64_t carry = 0;
@@ -762,9 +781,13 @@ __global__ void __launch_bounds__(128, 1) k_rns_crt_mma(RnsCrt a, RnsTables tb) 
             store_rounded<L, NX>(a.cm, a.ce, a.cplane, e, x, z ? EZ : Ea + Eb);
         }
     }
-    if (threadIdx.x == 0 && fail_sh) {
-        if (!mbar_wait(&bar_load, 0, kWaitLimit)) fail_sh = 3;
-        else if (fail_sh == 2 && !mbar_wait(&bar_mma, 0, kWaitLimit)) fail_sh = 4;
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();                                      // TMEM read out before the next tile's MMAs
+    }
+    if (threadIdx.x == 0 && fail_sh) {                    // bounded drain of our own copies and MMAs
+        for (int q = waited; q < issued; q++)
+            if (!mbar_wait(&bar_load, q & 1, kWaitLimit)) { fail_sh = 3; break; }
+        if (fail_sh != 3 && mma_pending && !mbar_wait(&bar_mma, (waited - 1) & 1, kWaitLimit)) fail_sh = 4;
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
@@ -901,7 +924,16 @@ int RnsLaunch<L>::crt_mma(const RnsCrt& a, const RnsTables& tb, cudaStream_t st)
         configured = true;
     }
     if (a.n == 0) return 0;
-    k_rns_crt_mma<L><<<(unsigned)((a.n + 127) / 128), 128, smem, st>>>(a, tb);
+    static int sms = 0;
+    if (!sms) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (sms <= 0) sms = 148;
+    }
+    const int64_t tiles = (a.n + 127) / 128;
+    const int64_t ctas = tiles < (int64_t)sms ? tiles : (int64_t)sms;     // persistent, one CTA per SM (TMEM 512)
+    k_rns_crt_mma<L><<<(unsigned)ctas, 128, smem, st>>>(a, tb);
     return (int)cudaGetLastError();
 }
 #endif
