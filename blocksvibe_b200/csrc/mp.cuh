@@ -91,7 +91,24 @@ template <int N> B3D_HD int bitlen(const u32 (&a)[N]) {
     return bl;
 }
 
-// out = floor(in / 2^sh), low NO limbs (sh >= 0; any size)
+// funnel shifts: low 32 bits of (hi:lo) >> b and high 32 bits of (hi:lo) << b, for 0 <= b < 32
+B3D_HD u32 fsr(u32 lo, u32 hi, int b) {
+#ifdef __CUDA_ARCH__
+    return __funnelshift_r(lo, hi, b);
+#else
+    return b ? ((lo >> b) | (hi << (32 - b))) : lo;
+#endif
+}
+
+B3D_HD u32 fsl(u32 lo, u32 hi, int b) {
+#ifdef __CUDA_ARCH__
+    return __funnelshift_l(lo, hi, b);
+#else
+    return b ? ((hi << b) | (lo >> (32 - b))) : hi;
+#endif
+}
+
+// out = floor(in / 2^sh), low NO limbs (sh >= 0; any size).  Shifts below one word skip the word stages.
 template <int NI, int NO> B3D_HD void shr(const u32 (&in)[NI], int sh, u32 (&out)[NO]) {
     constexpr int NT = (NI > NO + 1 ? NI : NO + 1);
     u32 t[NT];
@@ -99,39 +116,37 @@ template <int NI, int NO> B3D_HD void shr(const u32 (&in)[NI], int sh, u32 (&out
     for (int k = 0; k < NT; k++) t[k] = k < NI ? in[k] : 0u;
     int w = sh >> 5, b = sh & 31;
     if (w >= NI) { zero(out); return; }
+    if (w) {
 #pragma unroll
-    for (int s = 1; s < NT; s <<= 1) {
-        if (w & s) {
+        for (int s = 1; s < NT; s <<= 1) {
+            if (w & s) {
 #pragma unroll
-            for (int k = 0; k < NT; k++) t[k] = (k + s < NT) ? t[k + s] : 0u;
+                for (int k = 0; k < NT; k++) t[k] = (k + s < NT) ? t[k + s] : 0u;
+            }
         }
     }
 #pragma unroll
-    for (int k = 0; k < NO; k++) {
-        u32 lo = t[k], hi = (k + 1 < NT) ? t[k + 1] : 0u;
-        out[k] = b ? ((lo >> b) | (hi << (32 - b))) : lo;
-    }
+    for (int k = 0; k < NO; k++) out[k] = fsr(t[k], (k + 1 < NT) ? t[k + 1] : 0u, b);
 }
 
-// out = (in * 2^sh) mod 2^(32 NO)  (sh >= 0)
+// out = (in * 2^sh) mod 2^(32 NO)  (sh >= 0).  Shifts below one word skip the word stages.
 template <int NI, int NO> B3D_HD void shl(const u32 (&in)[NI], int sh, u32 (&out)[NO]) {
     u32 t[NO];
 #pragma unroll
     for (int k = 0; k < NO; k++) t[k] = k < NI ? in[k] : 0u;
     int w = sh >> 5, b = sh & 31;
     if (w >= NO) { zero(out); return; }
+    if (w) {
 #pragma unroll
-    for (int s = 1; s < NO; s <<= 1) {
-        if (w & s) {
+        for (int s = 1; s < NO; s <<= 1) {
+            if (w & s) {
 #pragma unroll
-            for (int k = NO - 1; k >= 0; k--) t[k] = (k - s >= 0) ? t[k - s] : 0u;
+                for (int k = NO - 1; k >= 0; k--) t[k] = (k - s >= 0) ? t[k - s] : 0u;
+            }
         }
     }
 #pragma unroll
-    for (int k = NO - 1; k >= 0; k--) {
-        u32 hi = t[k], lo = (k > 0) ? t[k - 1] : 0u;
-        out[k] = b ? ((hi << b) | (lo >> (32 - b))) : hi;
-    }
+    for (int k = NO - 1; k >= 0; k--) out[k] = fsl((k > 0) ? t[k - 1] : 0u, t[k], b);
 }
 
 // load one element of a limb-plane array as sign + magnitude
@@ -304,11 +319,18 @@ template <int L> B3D_HD void add_norm(const u32 (&a)[L], bool na, i64 ea, const 
     u32 acc[L + 2];
     zero(acc);
     u32 t[L + 2];
-    i64 da = ea - T, db = eb - T;            // >= 0 means a left shift
-    if (da >= 0) shl(a, (int)da, t); else shr(a, (int)(-da > 64 * L ? 64 * L : -da), t);
-    add_signed(acc, t, na);
-    if (db >= 0) shl(b, (int)db, t); else shr(b, (int)(-db > 64 * L ? 64 * L : -db), t);
-    add_signed(acc, t, nb);
+    // the operand with the larger exponent moves up by exactly one word (no barrel shift); the other by
+    // 32 - (difference) bits
+    const bool abig = ea >= eb;
+    t[0] = 0;
+#pragma unroll
+    for (int k = 0; k < L; k++) t[k + 1] = abig ? a[k] : b[k];
+    t[L + 1] = 0;
+    add_signed(acc, t, abig ? na : nb);
+    const i64 ds = (abig ? eb : ea) - T;     // <= 32
+    const u32(&sm)[L] = abig ? b : a;
+    if (ds >= 0) shl(sm, (int)ds, t); else shr(sm, (int)(-ds > 64 * L ? 64 * L : -ds), t);
+    add_signed(acc, t, abig ? nb : na);
     bool neg = (acc[L + 1] >> 31) != 0;
     if (neg) negate(acc);
     if (!round_mag<L>(acc, T, r, er)) { *nr = false; return; }
