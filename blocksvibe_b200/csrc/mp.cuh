@@ -322,17 +322,33 @@ template <int L> B3D_HD void add_norm(const u32 (&a)[L], bool na, i64 ea, const 
     // the operand with the larger exponent moves up by exactly one word (no barrel shift); the other by
     // 32 - (difference) bits
     const bool abig = ea >= eb;
-    t[0] = 0;
-#pragma unroll
-    for (int k = 0; k < L; k++) t[k + 1] = abig ? a[k] : b[k];
-    t[L + 1] = 0;
-    add_signed(acc, t, abig ? na : nb);
+    const bool sbig = abig ? na : nb, ssmall = abig ? nb : na;
     const i64 ds = (abig ? eb : ea) - T;     // <= 32
     const u32(&sm)[L] = abig ? b : a;
     if (ds >= 0) shl(sm, (int)ds, t); else shr(sm, (int)(-ds > 64 * L ? 64 * L : -ds), t);
-    add_signed(acc, t, abig ? nb : na);
-    bool neg = (acc[L + 1] >> 31) != 0;
-    if (neg) negate(acc);
+    // magnitudes: |big| 2^32 +- |small|, one carry (or borrow) chain; a borrow out means |small| was larger
+    bool neg = sbig;
+    if (sbig == ssmall) {
+        u32 c = 0;
+#pragma unroll
+        for (int k = 0; k < L + 2; k++) {
+            const u64 v = (u64)(k >= 1 && k <= L ? (abig ? a[k - 1] : b[k - 1]) : 0u) + t[k] + c;
+            acc[k] = (u32)v;
+            c = (u32)(v >> 32);
+        }
+    } else {
+        u32 br = 0;
+#pragma unroll
+        for (int k = 0; k < L + 2; k++) {
+            const u64 v = (u64)(k >= 1 && k <= L ? (abig ? a[k - 1] : b[k - 1]) : 0u) - t[k] - br;
+            acc[k] = (u32)v;
+            br = (u32)(v >> 63);
+        }
+        if (br) {
+            negate(acc);
+            neg = !neg;
+        }
+    }
     if (!round_mag<L>(acc, T, r, er)) { *nr = false; return; }
     *nr = neg;
 }
