@@ -2,6 +2,7 @@
 // GEMM, the recursion's Cauchy and pole steps, and the derivative moments.  Every kernel is a template
 // over the limb count L; inst.cu instantiates the launchers once per L, abi.cu dispatches on L.
 #pragma once
+#include <type_traits>
 #include <cuda_runtime.h>
 
 #include "mp.cuh"
@@ -54,6 +55,46 @@ __global__ void k_align(const int32_t* __restrict__ m, const i64* __restrict__ e
         }
         store_signed<L>(om, oplane, dst, s, neg);
     }
+}
+
+// Exact sums of products, rounded once, computed in two tries (the pole steps).  The first drops the product columns below
+// trunc_cols<L>() (mac_signed_mem), which leaves the accumulator within 2^(32 (trunc_cols + 2)) of the exact sum;
+// where round_safe shows that no value that close rounds differently, its rounding is the exact sum's.  Elsewhere
+// (heavy cancellation, a sum at a rounding midpoint, exact zeros) the second try redoes the sum exactly.  With
+// both operands normalised a product has about 64 L bits and the rounding bit sits near bit 32 L, so the first
+// try has some 90 bits to spare.
+template <int L> B3D_CX int trunc_cols() { return L >= 10 ? L - 5 : 0; }
+
+// sum(std::integral_constant<int, C0>) fills the two's complement accumulator (limb w at acc[w * stride]) and
+// returns whether it added any product.  mag receives the magnitude of an accumulator whose rounding equals the
+// exact sum's; the return value is its sign.
+template <int L, int NW, class Sum> __device__ __forceinline__ bool exact_sum(Sum& sum, u32* acc, int stride,
+                                                                               u32 (&mag)[NW]) {
+    constexpr int C0 = trunc_cols<L>();
+    auto load = [&]() {
+#pragma unroll
+        for (int w = 0; w < NW; w++) mag[w] = acc[w * stride];
+        const bool neg = (mag[NW - 1] >> 31) != 0;
+        if (neg) negate(mag);
+        return neg;
+    };
+    const bool any = sum(std::integral_constant<int, C0>());
+    bool neg = load();
+    if (C0 > 0 && any && !round_safe<L, NW, C0 + 2>(mag)) {
+        sum(std::integral_constant<int, 0>());
+        neg = load();
+    }
+    return neg;
+}
+
+// Round a magnitude (NW limbs, value mag * 2^ein) and store it normalised with the given sign.
+template <int L, int NW> __device__ __forceinline__ void store_rounded_mag(int32_t* m, i64* e, i64 plane, i64 i,
+                                                                           const u32 (&mag)[NW], bool neg, i64 ein) {
+    u32 r[L];
+    i64 er;
+    if (!round_mag<L>(mag, ein, r, &er)) neg = false;
+    store_signed<L>(m, plane, i, r, neg);
+    e[i] = er;
 }
 
 // Batched product of aligned operands: C[b, i, j] = sum_k A[b, i, k] B[b, k, j] with A rows and B
@@ -455,26 +496,30 @@ __global__ void __launch_bounds__(kPoleThreads, 3) k_pole1(const int32_t* __rest
     constexpr int NW = 2 * L + 2;
     extern __shared__ u32 pole_acc[];                    // (NW, blockDim.x): this thread's column
     u32* acc = pole_acc + threadIdx.x;
+    auto sum = [&](auto cols) {                          // acc = the sum from product column cols up
 #pragma unroll
-    for (int w = 0; w < NW; w++) acc[w * kPoleThreads] = 0;
-    if (E != EZ && Er != EZ) {
+        for (int w = 0; w < NW; w++) acc[w * kPoleThreads] = 0;
+        bool any = false;
+        if (E != EZ && Er != EZ) {
 #pragma unroll 1
-        for (int b = 0; b < S; b++) {
-            u32 x[L], y[L], r[L];
-            bool nr = load_mag<L>(Rm, Rplane, (rk * S + b0) * S + b, r);
-            if (is_zero(r)) continue;
-            i64 ix = hb + b * B;
-            bool nx = load_mag<L>(hm, hplane, ix, x);
-            i64 ex = he[ix];
-            if (is_zero(x) || ex == EZ || E - ex >= 32 * L) continue;
-            shr(x, (int)(E - ex), y);
-            mac_signed_mem<L, NW>(acc, kPoleThreads, r, y, nr != nx);
+            for (int b = 0; b < S; b++) {
+                u32 x[L], y[L], r[L];
+                bool nr = load_mag<L>(Rm, Rplane, (rk * S + b0) * S + b, r);
+                if (is_zero(r)) continue;
+                i64 ix = hb + b * B;
+                bool nx = load_mag<L>(hm, hplane, ix, x);
+                i64 ex = he[ix];
+                if (is_zero(x) || ex == EZ || E - ex >= 32 * L) continue;
+                shr(x, (int)(E - ex), y);
+                mac_signed_mem<L, NW, decltype(cols)::value>(acc, kPoleThreads, r, y, nr != nx);
+                any = true;
+            }
         }
-    }
-    u32 accr[NW];
-#pragma unroll
-    for (int w = 0; w < NW; w++) accr[w] = acc[w * kPoleThreads];
-    store_rounded<L, NW>(ym, ye, yplane, idx, accr, (E == EZ || Er == EZ) ? EZ : E + Er);
+        return any;
+    };
+    u32 mag[NW];
+    const bool neg = exact_sum<L, NW>(sum, acc, kPoleThreads, mag);
+    store_rounded_mag<L, NW>(ym, ye, yplane, idx, mag, neg, (E == EZ || Er == EZ) ? EZ : E + Er);
 }
 
 // Pole step, stage 2: res[t_slot[t], a0, b0, k] = sum_a QL[a0, a] Y[t, a, b0, k]  (QL = QLtab[t_qL[t]]
@@ -499,27 +544,31 @@ __global__ void __launch_bounds__(kPoleThreads, 3) k_pole2(const int32_t* __rest
     constexpr int NW = 2 * L + 2;
     extern __shared__ u32 pole_acc[];                    // (NW, blockDim.x): this thread's column
     u32* acc = pole_acc + threadIdx.x;
+    auto sum = [&](auto cols) {                          // acc = the sum from product column cols up
 #pragma unroll
-    for (int w = 0; w < NW; w++) acc[w * kPoleThreads] = 0;
-    if (E != EZ && Eq != EZ) {
+        for (int w = 0; w < NW; w++) acc[w * kPoleThreads] = 0;
+        bool any = false;
+        if (E != EZ && Eq != EZ) {
 #pragma unroll 1
-        for (int a = 0; a < S; a++) {
-            u32 x[L], y[L], q[L];
-            bool nq = load_mag<L>(Qm, Qplane, (qk * S + a0) * S + a, q);
-            if (is_zero(q)) continue;
-            i64 ix = yb + a * S * B;
-            bool nx = load_mag<L>(ym, yplane, ix, x);
-            i64 ex = ye[ix];
-            if (is_zero(x) || ex == EZ || E - ex >= 32 * L) continue;
-            shr(x, (int)(E - ex), y);
-            mac_signed_mem<L, NW>(acc, kPoleThreads, q, y, nq != nx);
+            for (int a = 0; a < S; a++) {
+                u32 x[L], y[L], q[L];
+                bool nq = load_mag<L>(Qm, Qplane, (qk * S + a0) * S + a, q);
+                if (is_zero(q)) continue;
+                i64 ix = yb + a * S * B;
+                bool nx = load_mag<L>(ym, yplane, ix, x);
+                i64 ex = ye[ix];
+                if (is_zero(x) || ex == EZ || E - ex >= 32 * L) continue;
+                shr(x, (int)(E - ex), y);
+                mac_signed_mem<L, NW, decltype(cols)::value>(acc, kPoleThreads, q, y, nq != nx);
+                any = true;
+            }
         }
-    }
-    u32 accr[NW];
-#pragma unroll
-    for (int w = 0; w < NW; w++) accr[w] = acc[w * kPoleThreads];
+        return any;
+    };
+    u32 mag[NW];
+    const bool neg = exact_sum<L, NW>(sum, acc, kPoleThreads, mag);
     i64 out = t_slot[t] * S * S * B + (a0 * S + b0) * B + k;
-    store_rounded<L, NW>(rm, re, rplane, out, accr, (E == EZ || Eq == EZ) ? EZ : E + Eq);
+    store_rounded_mag<L, NW>(rm, re, rplane, out, mag, neg, (E == EZ || Eq == EZ) ? EZ : E + Eq);
 }
 
 // ------------------------------------------------------------------------------------------------

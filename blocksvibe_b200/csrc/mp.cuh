@@ -241,13 +241,16 @@ template <int L, int NW> B3D_HD void mac_signed(u32 (&acc)[NW], const u32 (&a)[L
 }
 
 // mac_signed with the accumulator in memory (limb k at acc[k * stride]; shared memory in the pole kernels, so
-// that the operands, not the 2 L + 2 accumulator limbs, occupy the registers): same result bit for bit
-template <int L, int NW> B3D_HD void mac_signed_mem(u32* acc, int stride, const u32 (&a)[L], const u32 (&b)[L],
-                                                    bool negative) {
+// that the operands, not the 2 L + 2 accumulator limbs, occupy the registers): same result bit for bit.
+// C0 > 0 scans only the columns from C0 up and leaves acc[0 .. C0) alone: the part of a * b it drops,
+// sum over x + y < C0 of a[x] b[y] 2^(32 (x + y)), lies in [0, C0 2^(32 (C0 + 1)) (1 + 2^-31)), so n such
+// products leave acc within n C0 2^(32 (C0 + 1)) (1 + 2^-31) < 2^(32 (C0 + 2)) of the exact sum (n C0 < 2^31).
+template <int L, int NW, int C0 = 0> B3D_HD void mac_signed_mem(u32* acc, int stride, const u32 (&a)[L],
+                                                                const u32 (&b)[L], bool negative) {
     u32 c0 = 0, c1 = 0, c2 = 0;
     i64 rc = 0;
 #pragma unroll
-    for (int col = 0; col < 2 * L; col++) {
+    for (int col = C0; col < 2 * L; col++) {
 #pragma unroll
         for (int x = 0; x < L; x++) {
             int y = col - x;
@@ -264,6 +267,40 @@ template <int L, int NW> B3D_HD void mac_signed_mem(u32* acc, int stride, const 
         acc[k * stride] = (u32)r;
         rc = r >> 32;
     }
+}
+
+// Whether round_mag gives the same result for w (an unsigned magnitude) and for every value within 2^(32 EW) of
+// it.  Rounding to NB bits, half away from zero, is constant between midpoints of the NB-bit grid, so it is
+// enough that no midpoint lies within the error: with hb the half bit of w (bit 0 of round_mag's shifted t),
+// the error must lie at least two bits below hb, and the bits of w in [32 EW, hb) must not be all zero when the
+// half bit is set (w just above a midpoint) nor all one when it is clear (w just below one).  The nearest
+// midpoint of the finer grid below 2^(bitlen - 1) is half a half-unit away, also out of reach.
+template <int L, int NW, int EW> B3D_HD bool round_safe(const u32 (&w)[NW]) {
+    constexpr int NB = nb_bits(L);
+    const int hb = bitlen(w) - NB - 1;
+    if (hb < 32 * EW + 2) return false;
+    u32 h = 0;
+#pragma unroll
+    for (int k = EW; k < NW; k++)
+        if (k == (hb >> 5)) h = (w[k] >> (hb & 31)) & 1u;
+    const u32 flip = h ? 0u : ~0u;
+    u32 any = 0;
+#pragma unroll
+    for (int k = EW; k < NW; k++) {
+        const int lo = 32 * k;
+        const u32 mask = hb >= lo + 32 ? ~0u : (hb > lo ? (1u << (hb - lo)) - 1u : 0u);
+        any |= (w[k] ^ flip) & mask;
+    }
+    return any != 0;
+}
+
+// round_safe for a two's complement accumulator (the rounding acts on its magnitude)
+template <int L, int NW, int EW> B3D_HD bool round_safe_signed(const u32 (&acc)[NW]) {
+    u32 w[NW];
+#pragma unroll
+    for (int k = 0; k < NW; k++) w[k] = acc[k];
+    if (w[NW - 1] >> 31) negate(w);
+    return round_safe<L, NW, EW>(w);
 }
 
 // acc (two's complement) += sgn * q, q an unsigned magnitude of NQ limbs (NQ <= NW)
