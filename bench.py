@@ -11,7 +11,8 @@ map.  Inputs are synthetic (random M matrices and h_infinity: the cost does not 
 The operator's constants (plan, M tables, derivative and write_output maps) are built once before timing,
 as they are once per group of tasks.  `value` times the step with h_inf already on the device; `e2e` times
 the same step through the drop-in runner's host interface: h_inf copied from pinned host memory and the
-write_output limbs copied back to the host inside the timed region.
+write_output limbs copied back to the host inside the timed region, every step (pipelined: a copy stream
+moves one step's results out and the next step's inputs in while a step runs).
 
 With N > 1 (torchrun), every rank runs the same workload on its own GPU (independent replicas: the path has no
 exchange step); the timing is the max over ranks and `value` counts the tasks of all ranks.
@@ -400,7 +401,10 @@ def run_ours(args):
     torch.cuda.synchronize()
     other_ms = max_over_ranks(s0.elapsed_time(s1) / args.steps, world, dev)
 
-    # end to end through the host interface, per-step latencies for p50 / p99
+    # end to end through the host interface.  Throughput: with the graph, the pipelined runner (every step's
+    # h_inf copied in from pinned host memory and its results copied out to pinned host memory, on a copy
+    # stream that overlaps the neighbouring steps); without it, one task at a time.  Latency (p50 / p99): one
+    # task at a time, copy in, step, copy out.
     for _ in range(args.warmup):
         step_e2e()
     torch.cuda.synchronize()
@@ -413,6 +417,18 @@ def run_ours(args):
         torch.cuda.synchronize()
         lat.append(time.perf_counter() - s)
     e2e_s = (time.perf_counter() - e0) / args.steps
+    e2e_mode = "one task at a time"
+    if graph is not None:
+        for _ in graph.run_stream([[t]] * args.warmup):
+            pass
+        torch.cuda.synchronize()
+        barrier(world)
+        e0 = time.perf_counter()
+        for host in graph.run_stream([[t]] * args.steps):
+            d2h[0] = sum(m.numel() * 4 + e.numel() * 8 for m, e in host.values())
+        torch.cuda.synchronize()
+        e2e_s = (time.perf_counter() - e0) / args.steps
+        e2e_mode = "pipelined (GraphStep.run_stream)"
     barrier(world)
     e2e_s = max_over_ranks(e2e_s, world, dev)
 
@@ -474,8 +490,9 @@ def run_ours(args):
                        "coordinates": list(c["coords"]), "rhs_per_task": len(ns), "parallelism": f"replicas{world}",
                        "l2": "inputs larger than L2 (residue slot buffer %.2f GB)" % (op.rec.footprint_bytes(len(ns)) / 1e9),
                        "cuda_graph": graph is not None},
-            "e2e": {"value": world / e2e_s, "unit": "tasks/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h[0]},
-            "latency_ms": {"p50": pct(0.5), "p99": pct(0.99), "source": "e2e steps"},
+            "e2e": {"value": world / e2e_s, "unit": "tasks/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h[0],
+                    "mode": e2e_mode},
+            "latency_ms": {"p50": pct(0.5), "p99": pct(0.99), "source": "e2e steps, one task at a time"},
             "gpu_launches": launches, "setup_s": t_setup,
             "other_schedule": {"schedule": "plain" if args.schedule == "batched" else "batched",
                                "value": world / (other_ms / 1e3), "ms_per_step": other_ms},

@@ -183,6 +183,79 @@ class GraphStep:
         self.graph.replay()
         return self.out
 
+    def _pipeline_buffers(self):
+        dev, L = self.op.device, self.op.L
+        copy = torch.cuda.Stream(dev)
+        stage = [self.stage, mpf.zeros(tuple(self.stage.shape), L, dev)]
+        outd = [{c: (torch.empty_like(x.m), torch.empty_like(x.e)) for c, x in self.out.items()} for _ in range(2)]
+        host = [{c: (torch.empty(x.m.shape, dtype=torch.int32, pin_memory=True),
+                     torch.empty(x.e.shape, dtype=torch.int64, pin_memory=True)) for c, x in self.out.items()}
+                for _ in range(2)]
+        in_ready = [torch.cuda.Event() for _ in range(2)]      # inputs of the slot are on the device
+        in_free = [torch.cuda.Event() for _ in range(2)]       # the step has taken them into the static input
+        out_ready = [torch.cuda.Event() for _ in range(2)]     # results copied out of the static output
+        host_ready = [torch.cuda.Event() for _ in range(2)]    # results on the host; the device copy is free
+        return copy, stage, outd, host, in_ready, in_free, out_ready, host_ready
+
+    def run_stream(self, batches):
+        """Pipelined replays.  For each list of host tasks (h_inf in pinned memory) taken from `batches`, yields
+        the results as pinned host arrays {coordinate: (m, e)}, in order; an item stays valid until the next
+        one is requested.  A copy stream moves batch i + 1's inputs in and batch i - 1's results out while
+        batch i's graph runs, so the host transfers overlap the step; the step's stream itself only adds two
+        device-to-device copies (inputs into the static buffer, results out of it).  Staging buffers, device
+        result copies and host buffers are double-buffered, every reuse ordered by an event; they are allocated on
+        the first call and kept for the next ones."""
+        dev = self.op.device
+        main = torch.cuda.current_stream(dev)
+        if getattr(self, "_pipe", None) is None:               # built once, reused by every call
+            self._pipe = self._pipeline_buffers()
+        copy, stage, outd, host, in_ready, in_free, out_ready, host_ready = self._pipe
+
+        def bring_in(j, tasks):
+            with torch.cuda.stream(copy):
+                copy.wait_event(in_free[j])
+                k = 0
+                for t in tasks:
+                    for n in self.ns:
+                        stage[j].m[:, k].copy_(t.h_inf[n].m, non_blocking=True)
+                        stage[j].e[k].copy_(t.h_inf[n].e, non_blocking=True)
+                        k += 1
+                in_ready[j].record(copy)
+
+        it = iter(batches)
+        nxt = next(it, None)
+        if nxt is None:
+            return
+        bring_in(0, nxt)
+        prev, i = None, 0
+        while nxt is not None:
+            j = i % 2
+            nxt = next(it, None)
+            if nxt is not None:
+                bring_in(1 - j, nxt)
+            main.wait_event(in_ready[j])
+            self.h.m.copy_(stage[j].m.permute(0, 2, 3, 4, 5, 1))
+            self.h.e.copy_(stage[j].e.permute(1, 2, 3, 4, 0))
+            in_free[j].record(main)
+            self.graph.replay()
+            main.wait_event(host_ready[j])
+            for c, x in self.out.items():
+                outd[j][c][0].copy_(x.m)
+                outd[j][c][1].copy_(x.e)
+            out_ready[j].record(main)
+            with torch.cuda.stream(copy):
+                copy.wait_event(out_ready[j])
+                for c in self.out:
+                    host[j][c][0].copy_(outd[j][c][0], non_blocking=True)
+                    host[j][c][1].copy_(outd[j][c][1], non_blocking=True)
+                host_ready[j].record(copy)
+            if prev is not None:
+                host_ready[prev].synchronize()
+                yield host[prev]
+            prev, i = j, i + 1
+        host_ready[prev].synchronize()
+        yield host[prev]
+
 
 def run_group(group, tasks, M, device="cuda", schedule="batched", max_rhs=None):
     """All tasks of one group on the GPU.  M: matrices for the plan's keys (dict of decimal strings or an MPF

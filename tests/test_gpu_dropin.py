@@ -141,3 +141,28 @@ def test_cuda_graph_step_equals_launched_step(cuda):
         got = g.run([task])
         for c in ref:
             assert torch.equal(ref[c].m, got[c].m) and torch.equal(ref[c].e, got[c].e), c
+
+
+def test_pipelined_stream_equals_replays(cuda):
+    """run_stream (inputs in and results out on a copy stream, overlapping the next replay) yields, batch by batch,
+    the bits of separate replays, also when a batch repeats and the double buffers wrap around"""
+    import dataclasses
+    G, tasks, M, _, _ = make_group(nq=3, seed=37, coords=("xt", "xt_radial"))
+    t = tasks[0]
+    ns = t.lambda_orders(G.Lambda)
+    op = DI.Operator(G, t.pp, t.parity, M, t.two_js_internal, list(t.coordinates), [t.delta_1_plus_2], cuda)
+    g = DI.GraphStep(op, 1, ns, t.delta_1_plus_2)
+    seq = [tasks[0], tasks[1], tasks[2], tasks[1], tasks[0]]
+    want = []
+    for task in seq:
+        out = g.run([task])
+        want.append({c: (x.m.cpu(), x.e.cpu()) for c, x in out.items()})
+    pinned = [dataclasses.replace(task, h_inf={n: mpf.MPF(h.m.pin_memory(), h.e.pin_memory())
+                                               for n, h in task.h_inf.items()}) for task in seq]
+    got = [{c: (m.clone(), e.clone()) for c, (m, e) in h.items()} for h in g.run_stream([[x] for x in pinned])]
+    assert len(got) == len(seq)
+    for w, r in zip(want, got):
+        assert w.keys() == r.keys()
+        for c in w:
+            assert torch.equal(w[c][0], r[c][0]) and torch.equal(w[c][1], r[c][1]), c
+    assert list(g.run_stream([])) == []
