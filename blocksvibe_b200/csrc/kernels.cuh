@@ -601,26 +601,35 @@ __global__ void __launch_bounds__(kMomThreads, 3) k_moments(const int32_t* __res
     u32 acc[NW];
 #pragma unroll
     for (int w = 0; w < NW; w++) acc[w] = accm[w * kMomThreads];
-    u32 y[L];
+    // y = n^kk x p between iterations lives in this thread's shared-memory column (free after the product,
+    // words [0, L)); add_norm_col reads it there and uses words [L, 2 L) as its scratch column
+    u32* ys = accm;
     i64 ey;
-    round_mag<L>(acc, ex + ep, y, &ey);
-    bool ny = nx != np;
-    i64 row = q_row[q];
+    {
+        u32 y[L];
+        round_mag<L>(acc, ex + ep, y, &ey);
+#pragma unroll
+        for (int k = 0; k < L; k++) ys[k * kMomThreads] = y[k];
+    }
+    const bool ny = nx != np;
+    const i64 row = q_row[q];
     for (int kk = 0; kk < R1; kk++) {
-        i64 o = (row * R1 + kk) * N + c;
-        u32 v[L], s[L];
-        bool nv = load_mag<L>(mm, mplane, o, v);
-        bool ns;
-        i64 es;
-        add_norm<L>(v, nv, me[o], y, ny, ey, s, &ns, &es);
-        store_signed<L>(mm, mplane, o, s, ns);
-        me[o] = es;
+        const i64 o = (row * R1 + kk) * N + c;
+        {
+            u32 v[L], s[L];
+            const bool nv = load_mag<L>(mm, mplane, o, v);
+            bool ns;
+            i64 es;
+            add_norm_col<L>(v, nv, me[o], ys, ny, ey, ys + L * kMomThreads, kMomThreads, s, &ns, &es);
+            store_signed<L>(mm, mplane, o, s, ns);
+            me[o] = es;
+        }
         if (kk + 1 < R1) {                             // y *= n (exact, then rounded)
-            u32 w[L + 1];
+            u32 w[L + 1], y[L];
             u64 carry = 0;
 #pragma unroll
             for (int k = 0; k < L; k++) {
-                u64 v2 = (u64)y[k] * (u64)nn + carry;
+                u64 v2 = (u64)ys[k * kMomThreads] * (u64)nn + carry;
                 w[k] = (u32)v2;
                 carry = v2 >> 32;
             }
@@ -631,6 +640,8 @@ __global__ void __launch_bounds__(kMomThreads, 3) k_moments(const int32_t* __res
             } else {
                 round_mag<L>(w, ey, y, &ey);
             }
+#pragma unroll
+            for (int k = 0; k < L; k++) ys[k * kMomThreads] = y[k];
         }
     }
 }

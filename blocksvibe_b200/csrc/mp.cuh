@@ -390,4 +390,82 @@ template <int L> B3D_HD void add_norm(const u32 (&a)[L], bool na, i64 ea, const 
     *nr = neg;
 }
 
+// add_norm with the second operand in memory (limb k at b[k * stride]; a shared-memory column in the moments
+// kernel) and a scratch column of L limbs (same stride): the same result bit for bit.  The smaller operand
+// is read from memory at a run-time word offset instead of going through the register barrel shifter: with
+// ds = 32 q + f (0 <= f < 32), word k of floor(|small| 2^ds) is fsl(S[k - q - 1], S[k - q], f), S[i] = 0
+// outside [0, L).  Fewer live registers, no shifter stages.
+template <int L> B3D_HD void add_norm_col(const u32 (&a)[L], bool na, i64 ea, const u32* b, bool nb, i64 eb,
+                                          u32* scratch, int stride, u32 (&r)[L], bool* nr, i64* er) {
+    u32 bor = 0;
+#pragma unroll
+    for (int k = 0; k < L; k++) bor |= b[k * stride];
+    const bool za = is_zero(a) || ea == EZ, zb = bor == 0 || eb == EZ;
+    if (za && zb) { zero(r); *nr = false; *er = EZ; return; }
+    if (za) {
+#pragma unroll
+        for (int k = 0; k < L; k++) r[k] = b[k * stride];
+        *nr = nb; *er = eb; return;
+    }
+    if (zb) {
+#pragma unroll
+        for (int k = 0; k < L; k++) r[k] = a[k];
+        *nr = na; *er = ea; return;
+    }
+    const i64 top = ea > eb ? ea : eb;
+    const i64 T = top - 32;
+    const bool abig = ea >= eb;
+    const bool sbig = abig ? na : nb, ssmall = abig ? nb : na;
+    const i64 ds = (abig ? eb : ea) - T;         // <= 32
+    const u32* S = b;
+    if (!abig) {                                 // the smaller operand is a: through the scratch column
+#pragma unroll
+        for (int k = 0; k < L; k++) scratch[k * stride] = a[k];
+        S = scratch;
+    }
+    const i64 dsc = ds < -64 * L ? -64 * L : ds;
+    const int q = (int)(dsc >= 0 ? dsc / 32 : -((-dsc + 31) / 32));     // floor(dsc / 32)
+    const int f = (int)(dsc - 32 * (i64)q);
+    u32 t[L + 2];
+    u32 lo = 0;
+    {
+        const int i = -q - 1;
+        lo = (i >= 0 && i < L) ? S[i * stride] : 0u;
+    }
+#pragma unroll
+    for (int k = 0; k < L + 2; k++) {
+        const int i = k - q;
+        const u32 hi = (i >= 0 && i < L) ? S[i * stride] : 0u;
+        t[k] = fsl(lo, hi, f);
+        lo = hi;
+    }
+    u32 acc[L + 2];
+    bool neg = sbig;
+    if (sbig == ssmall) {
+        u32 c = 0;
+#pragma unroll
+        for (int k = 0; k < L + 2; k++) {
+            const u32 big = (k >= 1 && k <= L) ? (abig ? a[k - 1] : b[(k - 1) * stride]) : 0u;
+            const u64 v = (u64)big + t[k] + c;
+            acc[k] = (u32)v;
+            c = (u32)(v >> 32);
+        }
+    } else {
+        u32 br = 0;
+#pragma unroll
+        for (int k = 0; k < L + 2; k++) {
+            const u32 big = (k >= 1 && k <= L) ? (abig ? a[k - 1] : b[(k - 1) * stride]) : 0u;
+            const u64 v = (u64)big - t[k] - br;
+            acc[k] = (u32)v;
+            br = (u32)(v >> 63);
+        }
+        if (br) {
+            negate(acc);
+            neg = !neg;
+        }
+    }
+    if (!round_mag<L>(acc, T, r, er)) { *nr = false; return; }
+    *nr = neg;
+}
+
 }  // namespace b3d
