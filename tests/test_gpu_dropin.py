@@ -63,8 +63,9 @@ def test_dropin_matches_oracle_chain(cuda):
     ("cfg2_shape_1024", dict(tj12=8, tj43=8, tjmax=4, order=6, Lam=3, precision=1024, kept=4, nq=1, coords=("xt",))),
 ])
 def test_worst_bits_per_config(cuda, name, args):
-    """the north star's bar: every output agrees with the oracle chain to more than prec - 8 bits (relative to
-    each polynomial's largest coefficient); the worst case is printed per configuration"""
+    """the drop-in bar (blocks_3d's outputs to 2^-(prec - 8)): every output agrees with the oracle chain to more
+    than prec - 8 bits (relative to each polynomial's largest coefficient); the worst case is printed per
+    configuration"""
     G, tasks, M, hstr, plan = make_group(**args)
     worst = chain_worst_bits(cuda, G, tasks, M, hstr, plan)
     print(f"\nworst-case agreement {name}: {worst:.1f} bits (precision {G.precision}, NB {32 * DI.limbs(G.precision) - 2})")
