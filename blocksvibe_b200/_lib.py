@@ -30,7 +30,14 @@ SIGNATURES = {
     "b3d_format_decimal": [_I, _P, _P, _Q, _Q, _P, _P, _P, _P, _P],
     "b3d_poly_sizes": [_I, _P, _P, _Q, _P, _Q, _I, _I, _P, _P, _P, _P],
     "b3d_emit_text": [_P, _I, _P, _P, _P, _P, _P, _P, _Q, _P, _P],
+    "b3d_plan_build": [_Q, _Q, _Q, _Q, _P, _I, _P],
+    "b3d_plan_scalars": [_P, _P],
+    "b3d_plan_keys": [_P, _P, _P, _P],
+    "b3d_plan_layout": [_P, _P, _P, _P],
+    "b3d_plan_level_dims": [_P, _Q, _P],
+    "b3d_plan_level": [_P, _Q, _P],
 }
+VOID = {"b3d_plan_destroy": [_P]}             # entry points without a status
 
 
 class LevelTables(ctypes.Structure):
@@ -72,6 +79,9 @@ def lib():
         for name, args in SIGNATURES.items():
             f = getattr(h, name)
             f.argtypes, f.restype = args, _I
+        for name, args in VOID.items():
+            f = getattr(h, name)
+            f.argtypes, f.restype = args, None
         h.b3d_last_error.argtypes, h.b3d_last_error.restype = [], ctypes.c_char_p
         _lib = h
     return _lib
@@ -86,4 +96,4 @@ def call(name, *args):
 
 
 def exported_symbols():
-    return ["b3d_last_error"] + list(SIGNATURES)
+    return ["b3d_last_error"] + list(SIGNATURES) + list(VOID)

@@ -25,7 +25,7 @@ def _nvcc():
 
 
 def _sources():
-    return [os.path.join(CSRC, f) for f in sorted(os.listdir(CSRC)) if f.endswith((".cu", ".cuh", ".h"))] + \
+    return [os.path.join(CSRC, f) for f in sorted(os.listdir(CSRC)) if f.endswith((".cu", ".cuh", ".h", ".cpp"))] + \
            [os.path.join(ROOT, "include", "b3dgpu.h")]
 
 
@@ -53,6 +53,8 @@ def build(force=False, verbose=False):
              "-o", os.path.join(BUILD, f"inst_L{L}.o")] for L in LIMBS]
     for unit in ("abi", "noalloc", "rns_mma", "json"):
         jobs.append([nvcc, *ARCH, *FLAGS, "-c", os.path.join(CSRC, f"{unit}.cu"), "-o", os.path.join(BUILD, f"{unit}.o")])
+    for unit in ("plan",):                               # host C++ (the recursion's index plan)
+        jobs.append([nvcc, *FLAGS, "-c", os.path.join(CSRC, f"{unit}.cpp"), "-o", os.path.join(BUILD, f"{unit}.o")])
     with ThreadPoolExecutor(max_workers=min(len(jobs), os.cpu_count() or 4)) as ex:
         for log in ex.map(_run, jobs):
             if verbose and log:

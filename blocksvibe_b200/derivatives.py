@@ -16,12 +16,12 @@ conformal_block_derivatives, restore_r_delta, shift_block, together_with_factors
 The moments v are accumulated during the recursion (one kernel per level, libb3dgpu b3d_moments_level);
 c, a, G, the polynomial part and the numerators are multiprecision GEMMs.  The numerator matrix
 A_j = [Pi_i(x) | Pi(x) (x + ub)^t] is exact: in y = 2x the roots are integers.  Pole shifting
-(kept_pole_order < order) replaces the unprotected poles by the kept ones with residues S a,
-S = A^-1 V (blocks_3d's shift_poles); its closed form S_ki = (y'_k / y_i)^h l_k(y_i) (l_k the Lagrange
-basis on the kept poles y', h = #kept // 2) is exact in rationals and folded into the numerator matrix.
+(kept_pole_order < order) replaces the unprotected poles by the kept ones (blocks_3d's shift_poles); the
+replaced pole's column has the closed form of numerator_basis_y, exact in rationals and folded into the
+numerator matrix.
 """
 from fractions import Fraction
-from math import comb, lcm
+from math import comb
 
 import mpmath as mp
 import numpy as np
@@ -31,80 +31,74 @@ from . import _lib, mpf, structure as S
 from .mpf import MPF
 
 
-# ---------------------------------------------------------------- exact integer polynomial helpers
+# ---------------------------------------------------------------- numerator basis (exact rationals)
 
-def poly_times_linear(p, a):
-    """p(y) (y + a), integer coefficients lowest first"""
-    out = [0] * (len(p) + 1)
-    for k, c in enumerate(p):
-        out[k] += a * c
-        out[k + 1] += c
-    return out
-
-
-def divide_by_roots(p, roots):
-    """[p(y) / (y - r) for r in roots], each r a root of p (exact synthetic division)"""
-    n = len(p) - 1
-    out = []
+def _poly_from_roots(roots):
+    """prod (y - r), coefficients lowest degree first"""
+    p = [Fraction(1)]
     for r in roots:
-        q, acc = [0] * n, 0
-        for k in range(n, 0, -1):
-            acc = p[k] + r * acc
-            q[k - 1] = acc
-        if p[0] + r * acc != 0:
-            raise ValueError("not a root")
-        out.append(q)
-    return out
+        p = [Fraction(0)] + p
+        for i in range(len(p) - 1):
+            p[i] -= r * p[i + 1]
+    return p
 
 
-def shifted_pole_columns(roots, new, comp):
-    """Numerator columns of blocks_3d's pole shifting, exact.  roots: old poles y_i = 2 x_i; new: the
-    protected old poles (y = 0) then the kept poles y'_k; comp[q] = Pi_new(y) / (y - new[q]).
-    Returns per old pole (polynomial numerator coefficients, positive integer denominator):
-    protected pole -> comp of its slot; unprotected pole i -> sum_k S_ki comp[nprot + k] with
-    S_ki = (y'_k / y_i)^h prod_{m != k} (y_i - y'_m) / (y'_k - y'_m), h = #kept // 2."""
-    nprot = sum(1 for y in new if y == 0)
-    keep = new[nprot:]
-    size = len(keep)
-    h = size // 2
-    dk = []
-    for k in range(size):
-        d = 1
-        for mm in range(size):
-            if mm != k:
-                d *= keep[k] - keep[mm]
-        dk.append(d)
-    common = 1
-    for d in dk:
-        common = lcm(common, abs(d))
-    weight = [keep[k] ** h * (common // abs(dk[k])) * (1 if dk[k] > 0 else -1) for k in range(size)]
-    ncoef = len(comp[0]) if comp else 1
-    cols = []
-    for y in roots:
-        if y == 0:
-            cols.append((list(comp[new.index(0)]), 1))
+def _deflate(p, r):
+    """(quotient, remainder) of p(y) by (y - r) (Horner)"""
+    q, acc = [Fraction(0)] * (len(p) - 1), Fraction(0)
+    for i in range(len(p) - 1, 0, -1):
+        acc = p[i] + r * acc
+        q[i - 1] = acc
+    return q, p[0] + r * acc if p else Fraction(0)
+
+
+def numerator_basis_y(tj, tj12, tj43, order, kept=None, R=0):
+    """The numerator basis of one spin in y = 2x (every pole position is then an integer y_i = 2 D_i - 2 ub):
+    (pole columns, polynomial columns, npj).  Pole column i multiplies the residue a_i of the i-th pole of the
+    spin at full order; polynomial column t = Pi(y) (y + 2 ub)^t multiplies the polynomial part; Pi is the
+    product over the output poles: the protected old poles (y = 0) and the kept ones (all other old poles
+    without pole shifting, else the nonzero poles of the block at kept_pole_order), npj of them.
+
+    Column of an old pole y_i, with Pi = y^z Pk(y) (z protected poles, Pk over the kept ones, h = #kept // 2):
+        y_i = 0:  Pi(y) / y
+        else:     y^z (Pk(y) - (y / y_i)^h Pk(y_i)) / (y - y_i)
+    Without pole shifting y_i is a root of Pk and this is Pi / (y - y_i).  With pole shifting it is blocks_3d's
+    replacement of the pole (shift_poles: residues A^-1 V a on the kept poles, A[r][k] = y'_k^(r - h),
+    V[r][i] = y_i^(r - h)): sum_k S_ki Pi / (y - y'_k) with S_ki = (y'_k / y_i)^h l_k(y_i), l_k the Lagrange
+    basis of the kept poles, which sums to the closed form above because y^h (h < #kept) is interpolated
+    exactly on the kept poles."""
+    two_ub = tj + 1 if tj <= 1 else tj + 2
+    ys = [S.twice_position(P, tj) - two_ub for P in S.block_poles(tj, tj12, tj43, order)]
+    pool = ys if kept is None else [S.twice_position(P, tj) - two_ub for P in S.block_poles(tj, tj12, tj43, kept)]
+    keep = [y for y in pool if y != 0]
+    z = ys.count(0)
+    h = len(keep) // 2
+    Pk = _poly_from_roots(keep)
+    Pi = [Fraction(0)] * z + Pk
+    pole_cols = []
+    for yi in ys:
+        if yi == 0:
+            pole_cols.append(Pi[1:])
             continue
-        if size == 0:
-            cols.append(([0] * ncoef, 1))
-            continue
-        poly = [0] * ncoef
-        for k in range(size):
-            f = weight[k]
-            for mm in range(size):
-                if mm != k:
-                    f *= y - keep[mm]
-            if f:
-                for c, v in enumerate(comp[nprot + k]):
-                    poly[c] += f * v
-        den = y ** h * common
-        if den < 0:
-            den, poly = -den, [-v for v in poly]
-        cols.append((poly, den))
-    return cols
+        c = sum(v * Fraction(yi) ** k for k, v in enumerate(Pk)) / Fraction(yi) ** h
+        N = list(Pk)
+        N[h] -= c
+        q, rem = _deflate(N, yi)
+        if rem != 0:
+            raise ArithmeticError("pole column is not a polynomial")
+        pole_cols.append([Fraction(0)] * z + q)
+    poly_cols, q = [], Pi
+    for t in range(R + 1):
+        poly_cols.append(q)
+        q = [Fraction(0)] + q
+        for i in range(len(q) - 1):
+            q[i] += two_ub * q[i + 1]
+    return pole_cols, poly_cols, z + len(keep)
 
 
-def _take_rows(X, idx):
-    return X.take(idx)
+def to_x(poly_y, scale):
+    """coefficients in x of 2^-scale p(2x)"""
+    return [v * Fraction(2) ** (k - scale) for k, v in enumerate(poly_y)]
 
 
 class Derivs:
@@ -131,36 +125,25 @@ class Derivs:
 
     # ------------------------------------------------------------ moment bookkeeping per level
     def _moment_levels(self):
-        pl, order, Jo, NP = self.plan, self.plan.order, self.Jo, self.NP
-        tjo = np.array(self.tjs, dtype=np.int64)
-        pos = {tj: jo for jo, tj in enumerate(self.tjs)}
+        """per level: (slots, moment rows, n) of the pole-step tasks whose spin is an output spin: the residue
+        of task (p, tj, pole) at level m feeds moment row (p Jo + jo) NP + i (i: the pole's index in the block at
+        full order) with weight n^k r_c^n, n = m + shift(pole)"""
+        pl, Jo, NP, dev = self.plan, self.Jo, self.NP, self.device
+        jo_of = np.full(pl.tjmax + 2 * pl.order + 3, -1, dtype=np.int64)
+        jo_of[np.array(self.tjs, dtype=np.int64)] = np.arange(Jo)
         self.levels = []
-        for m in range(order):
-            tjs = pl._tjs[m]
-            sel = np.flatnonzero(np.isin(tjs, tjo))
-            npol = pl._npol[m][sel]
-            tot = int(npol.sum())
-            if tot == 0:
+        for lev in pl.levels:
+            jo = None if lev is None else jo_of[lev["t_tj"]]
+            if jo is None or not (jo >= 0).any():
                 self.levels.append(None)
                 continue
-            rep = np.repeat(np.arange(len(sel)), npol)
-            pidx = np.arange(tot) - np.repeat(np.cumsum(npol) - npol, npol)
-            jidx = sel[rep]
-            tj = tjs[jidx]
-            jo = np.array([pos[int(x)] for x in tj], dtype=np.int64)
-            kind, k = S.pole_at_v(tj, pl.tj12, pl.tj43, pl._ords[m][jidx], pidx)
-            i = S.pole_index_v(tj, pl.tj12, pl.tj43, order, kind, k)
-            nn = m + S.level_shift_v(kind, k)
-            jidx, pidx, jo, i, nn = (np.repeat(a, 2) for a in (jidx, pidx, jo, i, nn))
-            p = np.tile(np.array([0, 1], dtype=np.int64), tot)
-            ph = pl.phys_slots(p * pl.nslots + pl._flat[pl._start[m] + jidx] + pidx)
-            ok = ph != pl.zero_slot
-            if not ok.any():
-                self.levels.append(None)
-                continue
-            dev = self.device
-            self.levels.append((torch.as_tensor(ph[ok], device=dev), torch.as_tensor(((p * Jo + jo) * NP + i)[ok], device=dev),
-                                torch.as_tensor(nn[ok].astype(np.int64), device=dev)))
+            sel = jo >= 0
+            tj, kind, k = lev["t_tj"][sel], lev["t_kind"][sel], lev["t_k"][sel]
+            i = S.pole_index_v(tj, pl.tj12, pl.tj43, pl.order, kind, k)
+            row = (lev["t_p"][sel] * Jo + jo[sel]) * NP + i
+            n = lev["m"] + S.level_shift_v(kind, k)
+            self.levels.append(tuple(torch.as_tensor(np.ascontiguousarray(a), dtype=torch.int64, device=dev)
+                                     for a in (lev["t_slot"][sel], row, n)))
 
     # ------------------------------------------------------------ constants (once per operator and R)
     def _constants(self):
@@ -171,59 +154,42 @@ class Derivs:
             self.rcpow = mpf.from_mp(pw, L, (order + 1,), dev)
             self.Wh = mpf.from_mp([(mp.mpf(n) ** k if (n or k) else 1) * pw[n] for k in range(R + 1) for n in range(order + 1)],
                                   L, (R + 1, order + 1), dev)
-        # C(e, k) D^(e-k) = C(e, k) d^(e-k) 2^(k-e) per distinct d = 2 D (index 0: zeros)
-        d2 = sorted({S.twice_position(P, tj) for tj, pl in zip(self.tjs, self.poles) for P in pl})
-        di = {d: q + 1 for q, d in enumerate(d2)}
-        ints, exps = [0] * (R + 1) ** 2, [0] * (R + 1) ** 2
-        for d in d2:
-            for e in range(R + 1):
-                ints += [comb(e, k) * d ** (e - k) if k <= e else 0 for k in range(R + 1)]
-                exps += [k - e for k in range(R + 1)]
-        self.Ttab = mpf.from_ints(ints, exps, L, (len(d2) + 1, R + 1, R + 1), dev)
+        # the shift of a polynomial in log r by a pole position D: T(D)[e][k] = C(e, k) D^(e - k), a Pascal matrix
+        # (T[e][k] = T[e-1][k-1] + D T[e-1][k]); one table per distinct position, row 0 of the table all zero
+        twice = [[S.twice_position(P, tj) for P in pl] for tj, pl in zip(self.tjs, self.poles)]
+        positions = np.unique(np.concatenate([np.array(t, dtype=np.int64) for t in twice]))
+        tables = [[Fraction(0)] * (R + 1) ** 2]
+        for d in positions.tolist():
+            D = Fraction(int(d), 2)
+            T = [[Fraction(0)] * (R + 1) for _ in range(R + 1)]
+            T[0][0] = Fraction(1)
+            for e in range(1, R + 1):
+                for k in range(e + 1):
+                    T[e][k] = (T[e - 1][k - 1] if k else 0) + D * T[e - 1][k]
+            tables.append([x for row in T for x in row])
+        self.Ttab = mpf.from_fractions([x for t in tables for x in t], L, (len(tables), R + 1, R + 1), dev)
         didx = np.zeros((Jo, NP), dtype=np.int64)
-        for jo, (tj, pl) in enumerate(zip(self.tjs, self.poles)):
-            didx[jo, :len(pl)] = [di[S.twice_position(P, tj)] for P in pl]
+        for jo, t in enumerate(twice):
+            didx[jo, :len(t)] = np.searchsorted(positions, t) + 1
         self.didx = torch.as_tensor(didx, device=dev)
         self._small_constants()
         self.Anum = self._numerator_matrix()
 
     def _numerator_matrix(self):
-        """A_j (Jo, Dout, NP + R + 1): columns Pi_i(x) (or the pole-shifted combinations), then
-        Pi(x) (x + ub)^t for t <= R; exact integers in y = 2x, rounded once"""
-        L, R, NP, Jo, Dout = self.L, self.R, self.NP, self.Jo, self.Dout
+        """A (Jo, Dout, NP + R + 1): per spin, the numerator basis (numerator_basis_y) in x, pole columns first
+        (padded to NP), then the R + 1 polynomial columns; exact rationals rounded once"""
+        R, NP, Jo, Dout = self.R, self.NP, self.Jo, self.Dout
         W = NP + R + 1
-        tj12, tj43 = self.plan.tj12, self.plan.tj43
-        vals = [Fraction(0)] * (Jo * Dout * W)
-        for jo, (tj, pl) in enumerate(zip(self.tjs, self.poles)):
-            two_ub = tj + 1 if tj <= 1 else tj + 2
-            roots = [S.twice_position(P, tj) - two_ub for P in pl]
-            if self.kept is None:
-                new = roots
-            else:
-                new = [y for y in roots if y == 0] + [S.twice_position(P, tj) - two_ub
-                                                      for P in S.block_poles(tj, tj12, tj43, self.kept)
-                                                      if S.twice_position(P, tj) != two_ub]
-            npj = len(new)
+        A = np.full((Jo, Dout, W), Fraction(0), dtype=object)
+        for jo, tj in enumerate(self.tjs):
+            poles, polys, npj = numerator_basis_y(tj, self.plan.tj12, self.plan.tj43, self.plan.order, self.kept, R)
             if npj + R + 1 > Dout:
                 raise ValueError(f"spin {tj}: {npj} poles after shifting exceed the output width")
-            Pi = [1]
-            for y0 in new:
-                Pi = poly_times_linear(Pi, -y0)
-            cols = []                                             # (column, integer poly, scale, denominator)
-            q = Pi
-            for t in range(R + 1):
-                cols.append((NP + t, q, npj + t, 1))
-                q = poly_times_linear(q, two_ub)
-            comp = divide_by_roots(Pi, new) if new else []
-            if self.kept is None:
-                cols += [(i, c, npj - 1, 1) for i, c in enumerate(comp)]
-            else:
-                cols += [(i, poly, npj - 1, den) for i, (poly, den) in enumerate(shifted_pole_columns(roots, new, comp))]
-            for col, poly, sc, den in cols:                       # x^k coefficient = poly[k] / den 2^(k - sc)
-                for k, v in enumerate(poly):
-                    if v:
-                        vals[(jo * Dout + k) * W + col] = Fraction(v, den) * Fraction(2) ** (k - sc)
-        return mpf.from_fractions(vals, L, (Jo, Dout, W), self.device)
+            for i, poly in enumerate(poles):
+                A[jo, :len(poly), i] = to_x(poly, npj - 1)
+            for t, poly in enumerate(polys):
+                A[jo, :len(poly), NP + t] = to_x(poly, npj + t)
+        return mpf.from_fractions(list(A.reshape(-1)), self.L, (Jo, Dout, W), self.device)
 
     def _small_constants(self):
         """R-dependent tables of the polynomial part: H[e][s] = sum_d C(e, d) G'[s][d] with

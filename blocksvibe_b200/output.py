@@ -100,56 +100,72 @@ def one_minus_prefactor_matrix(O):
     return P
 
 
+def binomial_products(N):
+    """P[a][b] = integer coefficients (lowest degree first) of (1 + t)^a (t - 1)^b, for a + b <= N"""
+    P = [[None] * (N + 1) for _ in range(N + 1)]
+    P[0][0] = [1]
+    for a in range(N + 1):
+        for b in range(N + 1 - a):
+            if a == b == 0:
+                continue
+            if b:
+                q = P[a][b - 1]                                 # times (t - 1)
+                P[a][b] = [(q[k - 1] if k else 0) - (q[k] if k < len(q) else 0) for k in range(len(q) + 1)]
+            else:
+                q = P[a - 1][0]                                 # times (1 + t)
+                P[a][0] = [(q[k - 1] if k else 0) + (q[k] if k < len(q) else 0) for k in range(len(q) + 1)]
+    return P
+
+
 def xt_map(O, p, D):
-    """(W (outputs x inputs) object array of mpf, inputs [(idx, e)], outputs [(n, b)]) for xt"""
+    """(W (outputs x inputs) object array of mpf, inputs [(idx, e)], outputs [(n, b)]) for xt, built by pulling
+    each output back through the chain (the adjoint of the step-by-step transforms).
+
+    With the full (both-triangle) matrices, Z = M F M^T, M = P(D/2) R_z S, and Z(j, i) = sigma Z(i, j):
+      output (n, b), m = p + 2 b, t = n + m:  xt = b!/m! sum_j c_j Z(t - j, j),  c_j = [u^j] (1 + u)^n (1 - u)^m
+      so xt = b!/m! sum_{a, c} Y(a, c) F(a, c)  with  Y(a, c) = sum_j c_j M[t - j][a] M[j][c];
+      input (idx, e), n' = p + 2 idx, s = n' + e, feeds only the antidiagonal a + c = s of F:
+      F(a, s - a) = 2^-s [t^e] (1 + t)^a (t - 1)^(s - a) for a >= s - a, sigma F(s - a, a) below it.
+    Every matrix is lower triangular, so no term crosses the truncation i + j <= O."""
     sigma = -1 if p % 2 else 1
     M = rho_to_z_matrix(O) * stirling_matrix(O)
     if D != 0:
         M = prefactor_matrix(O, D / 2) * M
-    Mv = [[M[i, k] for k in range(O + 1)] for i in range(O + 1)]
+    Mv = np.array([[M[i, k] for k in range(O + 1)] for i in range(O + 1)], dtype=object)
     inputs = [(idx, e) for idx in range((O - p) // 2 + 1) for e in range(O - (p + 2 * idx) + 1)]
     outputs = [(n, b) for n in range(O - p + 1) for b in range((O - n - p) // 2 + 1)]
-    K = len(inputs)
-    # Z(i, j) for i >= j, i + j <= O, as a linear form over the inputs
-    Z = {}
-    for (i, j) in ((i, j) for i in range(O + 1) for j in range(min(i, O - i) + 1)):
-        Z[(i, j)] = [mp.mpf(0)] * K
+    P = binomial_products(O)
+    # per antidiagonal s: the inputs feeding it and F(a, s - a) per input (rows a = 0..s)
+    feed = {}
     for u, (idx, e) in enumerate(inputs):
-        s = p + 2 * idx + e                                # antidiagonal of F fed by this input
-        f = []                                             # F(k, s - k), k = 0..s, full (sigma-symmetric)
-        for k in range(s + 1):
-            i, j = (k, s - k) if k >= s - k else (s - k, k)
-            if j > min(i, O - i):
-                f.append(mp.mpf(0))
-                continue
-            acc = 0
-            for a in range(max(0, e - j), min(i, e) + 1):
-                acc += (-1) ** (j - (e - a)) * math.comb(i, a) * math.comb(j, e - a)
-            v = mp.mpf(acc) / mp.mpf(2) ** s
-            f.append(v if k >= s - k else sigma * v)
-        for (i, j), row in Z.items():
-            if i + j < s:
-                continue
-            acc = mp.mpf(0)
-            for k in range(max(0, s - j), min(i, s) + 1):
-                if f[k]:
-                    acc += Mv[i][k] * Mv[j][s - k] * f[k]
-            row[u] = acc
-    W = np.empty((len(outputs), K), dtype=object)
+        s = p + 2 * idx + e
+        col = []
+        for a in range(s + 1):
+            hi, lo = max(a, s - a), min(a, s - a)
+            c = P[hi][lo]
+            v = mp.ldexp(c[e], -s) if e < len(c) else mp.mpf(0)
+            col.append(v if a >= s - a else sigma * v)
+        feed.setdefault(s, ([], []))
+        feed[s][0].append(u)
+        feed[s][1].append(col)
+    feed = {s: (us, np.array(cols, dtype=object).T) for s, (us, cols) in feed.items()}
+    W = np.empty((len(outputs), len(inputs)), dtype=object)
     W[:] = mp.mpf(0)
     for o, (n, b) in enumerate(outputs):
         m = p + 2 * b
-        fac = mp.factorial((m - p) // 2) / mp.factorial(m)
-        for jj in range(n + m + 1):                        # Z(n + m - jj, jj)
-            c = sum((-1) ** l * math.comb(n, jj - l) * math.comb(m, l)
-                    for l in range(max(0, jj - n), min(m, jj) + 1))
-            if not c:
+        t = n + m
+        cj = P[n][m] if m % 2 == 0 else [-x for x in P[n][m]]        # (1 + u)^n (1 - u)^m
+        Y = np.empty((t + 1, t + 1), dtype=object)
+        Y[:] = mp.mpf(0)
+        for j in range(t + 1):
+            if j < len(cj) and cj[j]:
+                Y[:t - j + 1, :j + 1] += cj[j] * np.outer(Mv[t - j, :t - j + 1], Mv[j, :j + 1])
+        fac = mp.factorial(b) / mp.factorial(m)
+        for s, (us, F) in feed.items():
+            if s > t:
                 continue
-            i, j = n + m - jj, jj
-            sgn = 1 if i >= j else sigma
-            row = Z[(i, j) if i >= j else (j, i)]
-            for u in range(K):
-                W[o, u] += fac * c * sgn * row[u]
+            anti = np.array([Y[a, s - a] for a in range(s + 1)], dtype=object)
+            W[o, us] = fac * anti.dot(F)
     return W, inputs, outputs
 
 

@@ -227,6 +227,43 @@ int b3d_pole_level_noalloc(int L, const int32_t* hm, const int64_t* he, int64_t 
                            const int64_t* t_hrow, const int64_t* t_R, const int64_t* t_qL, const int64_t* t_slot,
                            int64_t T, int64_t B, int S, int32_t* rm, int64_t* re, int64_t rplane, void* stream);
 
+/* ---- Index plan of the recursion (host memory; replaces the reference's recursion_gpu.Plan,
+ *      recursion_gpu.py:136-365, whose tensors it reproduces: logical slots (m, spin, pole) with parity p adding
+ *      p * nslots, per level the Cauchy groups (src, tj') with their rows D' and columns, per pole-step task its
+ *      slot, H row and keys, every numbering by first appearance, and LIFO slot recycling) ---- */
+
+typedef struct b3d_plan b3d_plan;
+
+/* number of int64 written by b3d_plan_scalars: Smax, Jh, nslots, nphys, zero_slot, dmax, order, number of M keys,
+ * of Q keys, of (L, Q) pairs, of (level, spin) layout entries */
+#define B3D_PLAN_NSCALARS 11
+
+/* Per-level arrays copied out by b3d_plan_level (int64, any pointer may be NULL to skip it).  With dims
+ * (nb, Mr, Kc, T) from b3d_plan_level_dims: gsrc, gj, nrow, ncol (nb); rowd (nb, Mr); col, cold (nb, Kc); per
+ * task (T): t_slot (physical), t_hrow (group * Mr + row), t_L / t_R (M key ids), t_q (Q key id), t_qL ((L, Q)
+ * pair id), t_p (parity), t_tj (doubled spin), t_kind / t_k (pole). */
+typedef struct b3d_plan_level_arrays {
+    int64_t *gsrc, *gj, *col, *rowd, *nrow, *cold, *ncol;
+    int64_t *t_slot, *t_hrow, *t_L, *t_R, *t_q, *t_qL, *t_p, *t_tj, *t_kind, *t_k;
+} b3d_plan_level_arrays;
+
+/* Build the plan of (two_j12, two_j43, two_j_max, order, pseudo_parities[2][2] as 4 int64), with slot recycling
+ * when reuse != 0 (reference Plan(..., reuse)).  *out is released with b3d_plan_destroy. */
+int b3d_plan_build(int64_t two_j12, int64_t two_j43, int64_t two_j_max, int64_t order, const int64_t* pseudo_parities,
+                   int reuse, b3d_plan** out);
+void b3d_plan_destroy(b3d_plan* plan);
+/* B3D_PLAN_NSCALARS values (above) */
+int b3d_plan_scalars(const b3d_plan* plan, int64_t* scalars);
+/* mkeys (nM, 5): kind, k, side (0 = L, 1 = R), pseudo-parity, two_j; qkeys (nQ, 4): kind, k, two_j, sign;
+ * lqpairs (nLQ, 2): M key id, Q key id; row i = id i (reference Plan.Mkeys / Qkeys / LQpairs) */
+int b3d_plan_keys(const b3d_plan* plan, int64_t* mkeys, int64_t* qkeys, int64_t* lqpairs);
+/* start (order) and first (layout entries): first logical slot of (m, spin index j) = first[start[m] + j];
+ * phys (2 nslots): physical slot of each logical one, -1 where never written */
+int b3d_plan_layout(const b3d_plan* plan, int64_t* start, int64_t* first, int64_t* phys);
+/* dims[4] = nb, Mr, Kc, T of level m (nb = 0: no task at that level) */
+int b3d_plan_level_dims(const b3d_plan* plan, int64_t m, int64_t* dims);
+int b3d_plan_level(const b3d_plan* plan, int64_t m, const b3d_plan_level_arrays* arrays);
+
 /* ---- blocks_3d's JSON output (reference blocksvibe/b3djson.py, called from cli._write_one, cli.py:471-490) ---- */
 
 /* Tables of the decimal formatter, built once per (L, p) by the caller: pow5 = 5^k for k = 0 .. kmax as rows of
