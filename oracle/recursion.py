@@ -10,54 +10,65 @@ import mpmath as mp
 from . import blocks as B
 
 
+def fill_level(h_inf, M, res, m, tj12, tj43, tj_max, order, pseudo_parities, jsel=None, t_end=None):
+    """the residues of level m (every spin index, or those in jsel), read from the residues of the levels
+    below in res; returns (new residues, MACs done, completed before t_end)"""
+    import time
+    zero = mp.mpf(0)
+    out, macs = {}, 0
+    for jidx, tj in enumerate(B.spins(m, order, tj12, tj_max)):
+        if jsel is not None and jidx not in jsel:
+            continue
+        for pidx, P in enumerate(B.pole_list(tj, tj12, tj43, order - m - B.excess(tj, tj_max))):
+            tjc = B.child(P, tj)
+            d_row = B.twice_pos(P, tj) + 2 * B.shift(P)
+            exc = B.excess(tjc, tj_max)
+            terms = []
+            for i in B.pole_list(tjc, tj12, tj43, m):
+                diff = d_row - B.twice_pos(i, tjc)
+                coef = mp.mpf(2) / diff if diff else zero
+                pos = B.pole_list(tjc, tj12, tj43, order - m + B.shift(i) - exc).index(i)
+                terms.append((m - B.shift(i), pos, coef))
+            q = B.q_value(P, tj)
+            qv = mp.mpf(q.numerator) / q.denominator
+            if (tjc - tj) % 4:
+                qv = -qv
+            for p in range(2):
+                src = (p + (1 if P[0] == 3 else 0)) % 2
+                left = M.get((P, 0, tj12, pseudo_parities[src][0], tj))
+                right = M.get((P, 1, tj43, pseudo_parities[src][1], tj))
+                if not left or not left[0] or not right or not right[0]:
+                    continue
+                nl, nr = len(left[0]), len(right[0])
+                jc = tjc // 2
+                h = [[h_inf.get((src, m, jc, a, b), zero)
+                      + mp.fsum(res.get((src, mm, jc, pos, a, b), zero) * c for mm, pos, c in terms)
+                      for b in range(nr)] for a in range(nl)]
+                for a0 in range(len(left)):
+                    for b0 in range(len(right)):
+                        out[(p, m, jidx, pidx, a0, b0)] = qv * mp.fsum(
+                            left[a0][a] * h[a][b] * right[b0][b] for a in range(nl) for b in range(nr))
+                macs += len(terms) * nl * nr + 2 * len(left) * len(right) * nl * nr
+            if t_end is not None and time.perf_counter() > t_end:
+                return out, macs, False
+    return out, macs, True
+
+
 def fill_residues(h_inf, M, tj12, tj43, tj_max, order, pseudo_parities, budget=None, stats=None):
     """budget: stop after this many seconds (a bounded sample for CPU timing); stats: dict receiving the
     multiprecision MACs done ("macs") and whether the run completed ("complete")"""
     import time
     t_end = None if budget is None else time.perf_counter() + budget
-    macs = 0
-    zero = mp.mpf(0)
+    macs, done = 0, True
     res = {}
     for m in range(order):
-        if t_end is not None and time.perf_counter() > t_end:
-            if stats is not None:
-                stats.update(macs=macs, complete=False)
-            return res
-        for jidx, tj in enumerate(B.spins(m, order, tj12, tj_max)):
-            for pidx, P in enumerate(B.pole_list(tj, tj12, tj43, order - m - B.excess(tj, tj_max))):
-                tjc = B.child(P, tj)
-                d_row = B.twice_pos(P, tj) + 2 * B.shift(P)
-                exc = B.excess(tjc, tj_max)
-                terms = []
-                for i in B.pole_list(tjc, tj12, tj43, m):
-                    diff = d_row - B.twice_pos(i, tjc)
-                    coef = mp.mpf(2) / diff if diff else zero
-                    pos = B.pole_list(tjc, tj12, tj43, order - m + B.shift(i) - exc).index(i)
-                    terms.append((m - B.shift(i), pos, coef))
-                q = B.q_value(P, tj)
-                qv = mp.mpf(q.numerator) / q.denominator
-                if (tjc - tj) % 4:
-                    qv = -qv
-                for p in range(2):
-                    src = (p + (1 if P[0] == 3 else 0)) % 2
-                    left = M.get((P, 0, tj12, pseudo_parities[src][0], tj))
-                    right = M.get((P, 1, tj43, pseudo_parities[src][1], tj))
-                    if not left or not left[0] or not right or not right[0]:
-                        continue
-                    nl, nr = len(left[0]), len(right[0])
-                    jc = tjc // 2
-                    h = [[h_inf.get((src, m, jc, a, b), zero)
-                          + mp.fsum(res.get((src, mm, jc, pos, a, b), zero) * c for mm, pos, c in terms)
-                          for b in range(nr)] for a in range(nl)]
-                    for a0 in range(len(left)):
-                        for b0 in range(len(right)):
-                            res[(p, m, jidx, pidx, a0, b0)] = qv * mp.fsum(
-                                left[a0][a] * h[a][b] * right[b0][b] for a in range(nl) for b in range(nr))
-                    macs += len(terms) * nl * nr + 2 * len(left) * len(right) * nl * nr
-                if t_end is not None and time.perf_counter() > t_end:
-                    break
+        new, n, done = fill_level(h_inf, M, res, m, tj12, tj43, tj_max, order, pseudo_parities, t_end=t_end)
+        res.update(new)
+        macs += n
+        if not done:
+            break
     if stats is not None:
-        stats.update(macs=macs, complete=t_end is None or time.perf_counter() <= t_end)
+        stats.update(macs=macs, complete=done)
     return res
 
 
