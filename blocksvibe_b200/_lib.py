@@ -36,6 +36,7 @@ SIGNATURES = {
     "b3d_plan_layout": [_P, _P, _P, _P],
     "b3d_plan_level_dims": [_P, _Q, _P],
     "b3d_plan_level": [_P, _Q, _P],
+    "b3d_setup_numbers": [_P, _Q, _I, _I, _P, _Q, _P],
 }
 VOID = {"b3d_plan_destroy": [_P]}             # entry points without a status
 

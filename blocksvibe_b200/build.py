@@ -53,7 +53,7 @@ def build(force=False, verbose=False):
              "-o", os.path.join(BUILD, f"inst_L{L}.o")] for L in LIMBS]
     for unit in ("abi", "noalloc", "rns_mma", "json"):
         jobs.append([nvcc, *ARCH, *FLAGS, "-c", os.path.join(CSRC, f"{unit}.cu"), "-o", os.path.join(BUILD, f"{unit}.o")])
-    for unit in ("plan",):                               # host C++ (the recursion's index plan)
+    for unit in ("plan", "setup_io"):                               # host C++ (the recursion's index plan)
         jobs.append([nvcc, *FLAGS, "-c", os.path.join(CSRC, f"{unit}.cpp"), "-o", os.path.join(BUILD, f"{unit}.o")])
     with ThreadPoolExecutor(max_workers=min(len(jobs), os.cpu_count() or 4)) as ex:
         for log in ex.map(_run, jobs):

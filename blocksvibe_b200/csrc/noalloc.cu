@@ -8,16 +8,21 @@
 // caller still owns and passes every input and output; only the intermediate product H R^T lives here.
 //
 // Limits and sharing rules:
-//  * the scratch is B3D_NOALLOC_SCRATCH_BYTES (16 MiB) of device memory, held by every GPU that loads the
-//    library until the process exits; a level needs T * S^2 * B * (4 L + 8) bytes (L-limb numbers and
-//    their exponents), larger requests are rejected with B3D_E_ARG and a message (split the level's tasks
-//    into chunks that fit);
+//  * the scratch is B3D_NOALLOC_SCRATCH_BYTES (16 MiB) of device memory, reserved on a device once this
+//    library's module is loaded there (with CUDA's lazy module loading, no later than the first call of this
+//    entry point on that device) and held until the process exits; a level needs T * S^2 * B * (4 L + 8)
+//    bytes (L-limb numbers and their exponents) and at most B3D_NOALLOC_SCRATCH_BYTES - 256 of them, larger
+//    requests are rejected with B3D_E_ARG and a message (split the level's tasks into chunks that fit);
 //  * every call on a device uses the same array, which keeps the last call's contents.  Nothing has to
 //    start at zero: the first kernel writes every scratch element the second kernel reads.  Calls whose
 //    kernels overlap on the GPU (different streams, or several host threads) race on the array: serialise
 //    them (one stream, or events);
-//  * the first call on each device looks up the array's device address (cudaGetSymbolAddress, with that
-//    device current) and caches it; make that first call before any stream capture begins.
+//  * the array is resolved on the CURRENT device (cudaGetDevice), not on the stream's: make the stream's device
+//    current before calling.  The first call on each device looks up the array's device address
+//    (cudaGetSymbolAddress) and caches it for the life of the process; make that first call before any stream
+//    capture begins.  A cudaDeviceReset (or any other teardown of the primary context) invalidates the cached
+//    address, and later calls in the same process would write through it: do not use this entry point in a
+//    process after resetting a device it has run on.
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -64,11 +69,15 @@ extern "C" int b3d_pole_level_noalloc(int L, const int32_t* hm, const int64_t* h
     if (!b3d_supported_limbs(L))
         return b3d::fail(B3D_E_LIMBS, "no kernels compiled for L = " + std::to_string(L));
     if (T == 0) return 0;
-    // scratch elements and bytes, checked against the array before any product can overflow
-    const uint64_t per = (uint64_t)S * (uint64_t)S * (uint64_t)B;
+    // scratch bytes T * S^2 * B * (4 L + 8), checked factor by factor so that no product can overflow
     const uint64_t num_bytes = 4u * (uint64_t)L + 8u;
     const uint64_t usable = kScratchBytes - 256;                  // room for aligning the exponent block
-    if ((uint64_t)T > usable / per / num_bytes)
+    const uint64_t row_bytes = (uint64_t)S * (uint64_t)S * num_bytes;          // <= 64 * 64 * 264
+    if ((uint64_t)B > usable / row_bytes)
+        return b3d::fail(B3D_E_ARG, "b3d_pole_level_noalloc: B = " + std::to_string(B) + " right-hand sides exceed the " +
+                                        std::to_string(kScratchBytes >> 20) + " MiB scratch even for one task");
+    const uint64_t per = (uint64_t)S * (uint64_t)S * (uint64_t)B;              // per * num_bytes <= usable
+    if ((uint64_t)T > usable / (per * num_bytes))
         return b3d::fail(B3D_E_ARG, "b3d_pole_level_noalloc: " + std::to_string(T) + " tasks x " + std::to_string(per) +
                                         " numbers of " + std::to_string(num_bytes) + " bytes exceed the " +
                                         std::to_string(kScratchBytes >> 20) + " MiB scratch; split the level");

@@ -6,7 +6,11 @@ and, per task, h_infinity for each lambda order (what the reference reads from b
 format ``cli._write_one`` hands to the JSON writer:
 
     {(q4, sign): (two_js, pp, {(coord, d12): (m (L, Jo, 2, S^2, outputs, Dmax) int32,
-                                              e (Jo, 2, S^2, outputs, Dmax) int64)}, outputs, Smax, 32 L - 2)}
+                                              e (Jo, 2, S^2, outputs, Dmax) int64)},
+                  {(coord, d12): OutputInfo}, Smax, 32 L - 2)}
+
+where OutputInfo.outputs lists the (derivative, derivative) pair of each output row, what the reference's
+writer reads (``cli._OutputInfo``, ``cli.py:443-447``, used by ``_write_one`` / ``_rows``, ``cli.py:471-498``).
 
 Two schedules over the same kernels:
   plain    one right-hand side batch per lambda order (all structures of a (pp, sign) subgroup), R = Lambda - n
@@ -14,7 +18,12 @@ Two schedules over the same kernels:
   batched  every (structure, lambda order) of a subgroup in ONE recursion pass (B = structures x orders),
            moments accumulated once with R = Lambda - parity, numerators finished per lambda order from the
            first R_n + 1 moments (the same sums: the moment of order k only depends on k).
+
+``gpu(tasks, q4s, sfile, mfile, timers)`` is the reference's ``cli._gpu`` itself (same arguments: the cli's
+Task objects, their (q4, sign) keys, b3d_setup's file and the cached M file; same result), reading the setup
+file with ``setup_file.read``.
 """
+import time
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -67,6 +76,24 @@ def limbs(precision):
     return mpf.limbs_for_precision(precision)
 
 
+class OutputInfo:
+    """what the JSON writer needs of a write_output map (host only, picklable): its output list"""
+
+    def __init__(self, outputs):
+        self.outputs = [tuple(o) for o in outputs]
+
+    def __repr__(self):
+        return f"OutputInfo({len(self.outputs)} outputs)"
+
+
+def task_results(tjs, pp, vals, infos, Smax, L, nq):
+    """per task q < nq of a batch: (two_js, pp, {(coord, d12): (m[..., q, :, :], e[..., q, :, :])}, infos, Smax,
+    32 L - 2) from host arrays vals[(coord, d12)] = (m (L, Jo, 2, S^2, nq, outputs, Dmax), e (Jo, 2, S^2, nq,
+    outputs, Dmax))"""
+    return [(tjs, pp, {k: (m[:, :, :, :, q], e[:, :, :, q]) for k, (m, e) in vals.items()}, infos, Smax, 32 * L - 2)
+            for q in range(nq)]
+
+
 class Operator:
     """Plan + recursion constants + derivative constants + write_output maps of one (pp, sign) subgroup,
     built once and reused for every batch (the reference rebuilds them per subgroup: cli.py:401-406)."""
@@ -75,6 +102,8 @@ class Operator:
         self.group, self.pp, self.parity = group, pp, parity
         self.L = limbs(group.precision)
         self.plan = Plan(group.two_j12, group.two_j43, group.two_j_max, group.order, pp, reuse=True)
+        if hasattr(M, "for_plan"):                      # a setup file's M table
+            M = M.for_plan(self.plan, device)
         self.rec = Recursion(self.plan, M, self.L, device=device)
         self.der = Derivs(self.plan, group.Lambda - parity, self.L, two_js=two_js,
                           kept_pole_order=group.kept_pole_order, device=device)
@@ -257,31 +286,92 @@ class GraphStep:
         yield host[prev]
 
 
-def run_group(group, tasks, M, device="cuda", schedule="batched", max_rhs=None):
-    """All tasks of one group on the GPU.  M: matrices for the plan's keys (dict of decimal strings or an MPF
-    table in plan.Mkeys order; per pseudo-parity subgroup: {pp: M}).  Returns the per-task host results
-    described in the module docstring."""
+def _d12s(task):
+    """a task's Delta_1+2 values (one string, or several for a structure written at more than one)"""
+    d = task.delta_1_plus_2
+    return list(d) if isinstance(d, (list, tuple)) else [d]
+
+
+def run_group(group, tasks, M, device="cuda", schedule="batched", max_rhs=None, timers=None):
+    """All tasks of one group on the GPU.  M: matrices for the plan's keys (dict of decimal strings, a setup
+    file's MTable, or an MPF table in plan.Mkeys order; per pseudo-parity subgroup: {pp: M}).  Returns the
+    per-task host results described in the module docstring; timers (a list) receives blocks_3d-style
+    (name, seconds, count) entries as the reference's _gpu records them."""
     sub = {}
     for t in tasks:
         sub.setdefault((tuple(t.pp), t.sign), []).append(t)
     results = {}
+    tick = lambda: (torch.cuda.synchronize(device), time.time())[1]
     for (pp, sign), ts in sub.items():
         parity = (1 - sign) // 2
         ns = sorted(set().union(*[t.lambda_orders(group.Lambda) for t in ts]))
         tjs = sorted(set().union(*[t.two_js_internal for t in ts]))
         coords = [c for c in ("xt", "xt_radial") if any(c in t.coordinates for t in ts)]
-        d12s = sorted({t.delta_1_plus_2 for t in ts})
+        d12s = sorted({d for t in ts for d in _d12s(t)})
+        t0 = tick()
         op = Operator(group, pp, parity, M[pp] if isinstance(M, dict) and pp in M else M, tjs, coords, d12s, device)
+        infos = {k: OutputInfo(o.outputs) for k, o in op.outs.items()}
+        t1 = tick()
         bmax = max_rhs or len(ts)
+        chain = out = 0.0
         for c0 in range(0, len(ts), bmax):
             ch = ts[c0:c0 + bmax]
+            s0 = tick()
             nums = op.run_batched(ch, ns) if schedule == "batched" else op.run_plain(ch, ns)
+            s1 = tick()
             vals = {}
             for d12 in d12s:
                 for c, (m, e) in op.to_host(op.apply_outputs(nums, d12)).items():   # (Jo, 2, S2, nq, outputs, Dmax)
                     vals[(c, d12)] = (m.numpy().copy(), e.numpy().copy())
-            for q, t in enumerate(ch):
-                results[(tuple(t.q4), t.sign)] = (
-                    tjs, pp, {k: (m[:, :, :, :, q], e[:, :, :, q]) for k, (m, e) in vals.items()},
-                    {k: list(o.outputs) for k, o in op.outs.items()}, op.plan.Smax, 32 * op.L - 2)
+            for t, r in zip(ch, task_results(tjs, pp, vals, infos, op.plan.Smax, op.L, len(ch))):
+                results[(tuple(t.q4), t.sign)] = r
+            chain += s1 - s0
+            out += tick() - s1
+        if timers is not None:
+            nb = -(-len(ts) // bmax)
+            timers += [(".main.gpu.constants", t1 - t0, 1), (".main.gpu.chain", chain, len(ns) * nb),
+                       (".main.gpu.write_output", out, 1)]
     return results
+
+
+def gpu(tasks, q4s, sfile, mfile, timers, device="cuda", schedule="batched"):
+    """The reference's ``cli._gpu`` (``cli.py:375-440``): tasks are the cli's Task objects of one group (two_js,
+    two_j12, two_j43, order, Lambda, tjmax, precision, kept_pole_order, delta_12, delta_43, two_js_internal,
+    coordinates, delta_1_plus_2, q4, sign), q4s their (q4, sign) keys, sfile b3d_setup's file and mfile the
+    cached M matrices (or None).  Returns {(q4, sign): (two_js, pp, {(coord, d12): (m, e)}, {(coord, d12):
+    OutputInfo}, Smax, 32 L - 2)}, the dict cli._write consumes."""
+    from . import setup_file
+    T = tasks[0]
+    L = limbs(T.precision)
+    t0 = time.time()
+    M, stasks = setup_file.read(sfile, L, m_path=mfile)
+    by_q4 = {(st.q4, st.sign): st for st in stasks}
+    timers.append((".main.gpu.read_setup", time.time() - t0, 1))
+    group = Group(tuple(T.two_js), T.two_j12, T.two_j43, T.order, T.Lambda, T.tjmax, T.precision,
+                  min(T.kept_pole_order, T.order), str(T.delta_12), str(T.delta_43))
+    wanted = {(tuple(q), s) for q, s in q4s}
+    runs = []
+    for t in tasks:
+        key = (tuple(t.q4), t.sign)
+        if key not in wanted or key not in by_q4 or any(key == (tuple(r.q4), r.sign) for r in runs):
+            continue
+        st = by_q4[key]
+        run = Task(key[0], t.sign, st.pp, list(t.two_js_internal), tuple(sorted(t.coordinates)), t.delta_1_plus_2)
+        runs.append(run)
+    # the subgroup's union of spins, coordinates and Delta_1+2 (as the reference computes it per subgroup)
+    for r in runs:
+        same = [t for t in tasks if t.sign == r.sign and by_q4.get((tuple(t.q4), t.sign)) is not None
+                and by_q4[(tuple(t.q4), t.sign)].pp == r.pp]
+        r.two_js_internal = sorted(set().union(*[t.two_js_internal for t in same]))
+        r.coordinates = tuple(c for c in ("xt", "xt_radial") if any(c in t.coordinates for t in same))
+        d12s = sorted({t.delta_1_plus_2 for t in same})
+        r.delta_1_plus_2 = d12s[0] if len(d12s) == 1 else tuple(d12s)
+    plans = {}
+    for r in runs:
+        key = r.pp
+        if key not in plans:
+            plans[key] = Plan(group.two_j12, group.two_j43, group.two_j_max, group.order, r.pp)
+        pl = plans[key]
+        for n in r.lambda_orders(group.Lambda):
+            r.h_inf[n] = by_q4[(tuple(r.q4), r.sign)].h_inf(n, group.order, pl.Jh, pl.Smax)
+    return run_group(group, runs, M, device=device, schedule=schedule, timers=timers)

@@ -212,7 +212,9 @@ int b3d_cauchy_add_hinf(int L, const int32_t* am, const int64_t* ae, int64_t apl
                         const int64_t* he, int64_t hplane, const b3d_level_tables* lv, int32_t* om, int64_t* oe,
                         int64_t oplane, void* stream);
 
-/* Size of the device scratch array of b3d_pole_level_noalloc (per GPU, held until the process exits). */
+/* Size of the device scratch array of b3d_pole_level_noalloc: reserved on a GPU once the library's module is
+ * loaded there (with lazy module loading, no later than the first b3d_pole_level_noalloc call on that GPU) and
+ * held until the process exits. */
 #define B3D_NOALLOC_SCRATCH_BYTES ((size_t)16 << 20)
 
 /* b3d_pole_level without a caller-provided scratch buffer (no counterpart in the reference: an addition for
@@ -220,8 +222,11 @@ int b3d_cauchy_add_hinf(int L, const int32_t* am, const int64_t* ae, int64_t apl
  * memory or a serving loop budgets it per request).  Same arguments and results as b3d_pole_level minus
  * ym / ye / yplane; the intermediate lives in a fixed array of B3D_NOALLOC_SCRATCH_BYTES, so a call needs
  * T * S^2 * B * (4 L + 8) <= B3D_NOALLOC_SCRATCH_BYTES - 256 bytes (else B3D_E_ARG: split the level's tasks).
- * Allocates nothing.  The first call on each device looks the array's address up: make it before any stream
- * capture.  All calls on a device share the array: calls whose kernels overlap on the GPU race. */
+ * Allocates nothing.  The array is resolved on the current device (make the stream's device current first); the
+ * first call on each device looks its address up and caches it for the life of the process: make that call
+ * before any stream capture, and do not call this entry point after a cudaDeviceReset of a device it ran on (the
+ * cached address is then stale).  All calls on a device share the array: calls whose kernels overlap on the GPU
+ * race. */
 int b3d_pole_level_noalloc(int L, const int32_t* hm, const int64_t* he, int64_t hplane, const int32_t* Rm,
                            const int64_t* Re, int64_t Rplane, const int32_t* Qm, const int64_t* Qe, int64_t Qplane,
                            const int64_t* t_hrow, const int64_t* t_R, const int64_t* t_qL, const int64_t* t_slot,
@@ -263,6 +268,14 @@ int b3d_plan_layout(const b3d_plan* plan, int64_t* start, int64_t* first, int64_
 /* dims[4] = nb, Mr, Kc, T of level m (nb = 0: no task at that level) */
 int b3d_plan_level_dims(const b3d_plan* plan, int64_t m, int64_t* dims);
 int b3d_plan_level(const b3d_plan* plan, int64_t m, const b3d_plan_level_arrays* arrays);
+
+/* ---- b3d_setup's file (csrc/b3d_setup.cxx:15-21 layout, read by the reference's setup.read, setup.py:128-161) ---- */
+
+/* Host memory.  n numbers of the file, records rec[i * (2 + K) ...] = [size, exp, limb_0 .. limb_{K-1}] (GMP mpf:
+ * 64-bit limbs, value sign(size) * sum_t limb_t 2^(64 t) * 2^(64 (exp - K))), rounded once to L limbs (half away
+ * from zero): limbs m[k * plane + i], exponents e[i] (B3D_EZ for zero).  Replaces setup.numbers_to_mpf
+ * (setup.py:52-74). */
+int b3d_setup_numbers(const int64_t* rec, int64_t n, int K, int L, int32_t* m, int64_t plane, int64_t* e);
 
 /* ---- blocks_3d's JSON output (reference blocksvibe/b3djson.py, called from cli._write_one, cli.py:471-490) ---- */
 

@@ -5,7 +5,7 @@ mpmath port of blocks_3d's fill_residues), recursion_gpu.Plan (the index plan), 
 write_output maps, derivatives._shift_columns (pole shifting), and the mpmath ports inside the
 reference's tests (tests/test_blocks_derivatives.reference, tests/test_blocks_output.reference_xt).
 
-    python tests/golden/make_golden.py [REFERENCE]
+    python tests/golden/make_golden.py REFERENCE
 
 Fixtures (all seed-fixed):
   plan.npz              Plan tensors for 7 + 1 operator shapes, with and without slot reuse
@@ -23,7 +23,9 @@ import types
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REFERENCE = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+if len(sys.argv) != 2:
+    sys.exit(__doc__)
+REFERENCE = sys.argv[1]
 
 
 def _import_reference():

@@ -10,7 +10,7 @@ b3djson imports gmpy2 (absent here) for its MPFR path only; an empty stand-in mo
 MPFR path prints the same strings except for values exactly halfway between two p-digit decimals, which
 these seeded values do not contain.
 
-    python tests/golden/make_json_golden.py [REFERENCE]
+    python tests/golden/make_json_golden.py REFERENCE
 """
 import json
 import os
@@ -19,7 +19,9 @@ import tempfile
 import types
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REFERENCE = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+if len(sys.argv) != 2:
+    sys.exit(__doc__)
+REFERENCE = sys.argv[1]
 sys.path.insert(0, REFERENCE)
 sys.path.insert(0, HERE)
 sys.modules.setdefault("gmpy2", types.ModuleType("gmpy2"))

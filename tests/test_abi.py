@@ -70,3 +70,16 @@ def test_kernels_refuse_cpu_tensors():
     X = mpf.zeros((3, 3), 10)
     with pytest.raises(_lib.B3DError):
         mpf.gemm(X, X)
+
+
+def test_noalloc_refuses_oversized_batches_before_touching_the_device():
+    """b3d_pole_level_noalloc checks T S^2 B (4 L + 8) against its fixed array factor by factor: a huge B (whose
+    product with S^2 would wrap in 64 bits) and a huge T are refused with B3D_E_ARG before any CUDA call, so this
+    runs without a GPU"""
+    lib = _lib.lib()
+    null = None
+    for T, B, S in ((1, 1 << 52, 64), (1, (1 << 63) - 1, 64), (1 << 40, 1, 5), (2, 1 << 20, 5)):
+        rc = lib.b3d_pole_level_noalloc(10, null, null, 0, null, null, 0, null, null, 0, null, null, null, null,
+                                        T, B, S, null, null, 0, null)
+        assert rc == -2, (T, B, S)
+        assert b"scratch" in lib.b3d_last_error()

@@ -61,6 +61,14 @@ def test_dropin_matches_oracle_chain(cuda):
                              coords=("xt_radial",), sign=-1)),
     ("cfg2_shape_512", dict(tj12=8, tj43=8, tjmax=8, order=8, Lam=5, precision=512, kept=5, nq=1, coords=("xt",))),
     ("cfg2_shape_1024", dict(tj12=8, tj43=8, tjmax=4, order=6, Lam=3, precision=1024, kept=4, nq=1, coords=("xt",))),
+    # the other limb counts the benchmarks run: 768 / 896 bits (644-task set, L = 26 / 30) and 1280 bits (serving
+    # stream and largest configuration, L = 42), each with pole shifting and both coordinates
+    ("set644_768", dict(tj12=4, tj43=4, tjmax=4, order=8, Lam=5, precision=768, kept=5, nq=1,
+                        coords=("xt", "xt_radial"), d12="0.7")),
+    ("set644_896_odd", dict(tj12=2, tj43=2, tjmax=6, order=8, Lam=5, precision=896, kept=6, nq=1,
+                            coords=("xt", "xt_radial"), sign=-1, pp=((0, 1), (1, 0)))),
+    ("cfg5_1280", dict(tj12=8, tj43=8, tjmax=4, order=7, Lam=4, precision=1280, kept=5, nq=1,
+                       coords=("xt", "xt_radial"), d12="6")),
 ])
 def test_worst_bits_per_config(cuda, name, args):
     """the drop-in bar (blocks_3d's outputs to 2^-(prec - 8)): every output agrees with the oracle chain to more
@@ -167,3 +175,38 @@ def test_pipelined_stream_equals_replays(cuda):
         for c in w:
             assert torch.equal(w[c][0], r[c][0]) and torch.equal(w[c][1], r[c][1]), c
     assert list(g.run_stream([])) == []
+
+
+def test_cli_gpu_entry_reads_setup_file(cuda, tmp_path):
+    """dropin.gpu, the reference's cli._gpu (same arguments: the cli's tasks, (q4, sign) keys, b3d_setup's file),
+    on a setup file holding a group's M matrices and h_inf: the results of run_group on the same numbers, bit for
+    bit, in the form the reference's writer consumes (OutputInfo objects with .outputs)"""
+    from types import SimpleNamespace
+    from blocksvibe_b200 import setup_file as SF
+    G, tasks, M, hstr, plan = make_group(nq=2, seed=41, coords=("xt", "xt_radial"))
+    L = DI.limbs(G.precision)
+    K = (32 * L + 64) // 64 + 2
+    with mp.workprec(32 * L + 64):
+        mats = {key: [[mp.mpf(x) for x in row] for row in rows] for key, rows in M.items()}
+        stasks = []
+        for q, t in enumerate(tasks):
+            h = {n: [tuple(ent[1:6]) + (mp.mpf(ent[6]),) for ent in hstr[(q, n)]] for n in t.lambda_orders(G.Lambda)}
+            stasks.append((t.q4, t.sign, t.pp, h))
+    sfile = str(tmp_path / "setup.bin")
+    SF.write(sfile, K, mats, stasks)
+    cli_tasks = [SimpleNamespace(two_js=list(G.two_js), two_j12=G.two_j12, two_j43=G.two_j43, order=G.order,
+                                 Lambda=G.Lambda, tjmax=G.two_j_max, precision=G.precision,
+                                 kept_pole_order=G.kept_pole_order, delta_12=G.delta_12, delta_43=G.delta_43,
+                                 two_js_internal=list(t.two_js_internal), coordinates=set(t.coordinates),
+                                 delta_1_plus_2=t.delta_1_plus_2, q4=list(t.q4), sign=t.sign) for t in tasks]
+    timers = []
+    got = DI.gpu(cli_tasks, [(tuple(t.q4), t.sign) for t in tasks], sfile, None, timers, device=cuda)
+    want = DI.run_group(G, tasks, M, device=cuda)
+    assert got.keys() == want.keys()
+    for k in want:
+        tjs, pp, vals, infos, Smax, NB = got[k]
+        assert (tjs, pp, Smax, NB) == (want[k][0], want[k][1], want[k][4], want[k][5])
+        assert {c: i.outputs for c, i in infos.items()} == {c: i.outputs for c, i in want[k][3].items()}
+        for c in want[k][2]:
+            assert np.array_equal(vals[c][0], want[k][2][c][0]) and np.array_equal(vals[c][1], want[k][2][c][1]), c
+    assert {name for name, _, _ in timers} >= {".main.gpu.read_setup", ".main.gpu.constants", ".main.gpu.chain"}

@@ -147,3 +147,23 @@ def test_write_files(cuda, tmp_path):
     w.write(outs, lambda tj: str(tmp_path / f"spin_{tj}.json"))
     for tj in opts.two_js_internal:
         assert (tmp_path / f"spin_{tj}.json").read_text() == g["files"][str(tj)]
+
+
+@pytest.mark.parametrize("ci", range(len(JC.SPIN_CASES)))
+def test_spinwriter_matches_reference_consumer_of_dropin_results(cuda, ci):
+    """the GPU writer on the device form of the drop-in's results (two tasks in one batch) gives the files the
+    reference's cli._write wrote from the host form of the same results (tests/golden/dropin_write.json)"""
+    from types import SimpleNamespace
+    import dropin_cases as DC
+    g = golden("dropin_write.json")[ci]
+    case = JC.SPIN_CASES[ci]
+    vals, outputs, Sm, L = DC.host_values(case)
+    outs = {c: mpf.MPF(torch.from_numpy(m).to(cuda), torch.from_numpy(e).to(cuda)) for c, (m, e) in vals.items()}
+    Dmax = case[8]
+    for q in range(len(DC.Q4S)):
+        attrs = dict(g["tasks"][q])
+        attrs["coordinates"] = set(attrs["coordinates"])
+        opts = SimpleNamespace(**attrs)
+        w = JO.SpinWriter(opts, sorted(opts.two_js_internal), case[4], outputs, Sm, len(DC.Q4S), Dmax, cuda)
+        files = {tj: bytes(v).decode() for tj, v in w.render(outs, q).items()}
+        assert files == {int(tj): t for tj, t in g["files"][str(q)].items()}

@@ -68,3 +68,42 @@ def test_noalloc_rejects_levels_beyond_its_scratch(cuda):
     assert b"scratch" in lib.b3d_last_error()
     torch.cuda.synchronize()
     assert torch.equal(before, res.e)
+
+
+def _synthetic_level(cuda, L, S, T, B, rows=64, keys=7, seed=6):
+    """random pole-step operands of T tasks (no plan needed): H rows, row-aligned R and q L tables, task maps"""
+    g = torch.Generator().manual_seed(seed)
+    H = mpf.random_mpf((rows, S * S * B), L, spread=4, device=cuda, generator=g)
+    Ra = mpf.align_rows(mpf.random_mpf((keys, S, S), L, spread=2, device=cuda, generator=g))
+    Qa = mpf.align_rows(mpf.random_mpf((keys, S, S), L, spread=2, device=cuda, generator=g))
+    idx = lambda hi: torch.randint(0, hi, (T,), generator=g).to(cuda)
+    return H, Ra, Qa, idx(rows), idx(keys), idx(keys), torch.arange(T, device=cuda)
+
+
+def test_noalloc_at_its_size_limit(cuda):
+    """a level needing exactly B3D_NOALLOC_SCRATCH_BYTES - 256 bytes of scratch (T S^2 B (4 L + 8) with L = 10,
+    S = 4, T = 257, B = 85) runs and equals b3d_pole_level bit for bit; one task more is refused"""
+    L, S, T, B = 10, 4, 257, 85
+    assert T * S * S * B * (4 * L + 8) == (16 << 20) - 256
+    H, Ra, Qa, hrow, tR, tq, slot = _synthetic_level(cuda, L, S, T + 1, B)
+    stream = torch.cuda.current_stream(cuda).cuda_stream
+    lib = _lib.lib()
+
+    def args(n, res):
+        return [_p(H.m), _p(H.e), H.m.stride(0), _p(Ra[0]), _p(Ra[1]), Ra[0].stride(0), _p(Qa[0]), _p(Qa[1]),
+                Qa[0].stride(0), _p(hrow), _p(tR), _p(tq), _p(slot), n, B, S]
+    ref = mpf.zeros((T + 2, S * S, B), L, cuda)
+    got = mpf.zeros((T + 2, S * S, B), L, cuda)
+    Y = mpf.zeros((T, S * S, B), L, cuda)
+    _lib.call("b3d_pole_level", L, *args(T, ref), _p(Y.m), _p(Y.e), Y.m.stride(0), _p(ref.m), _p(ref.e),
+              ref.m.stride(0), stream)
+    rc = lib.b3d_pole_level_noalloc(L, *args(T, got), _p(got.m), _p(got.e), got.m.stride(0), stream)
+    assert rc == 0, lib.b3d_last_error().decode()
+    torch.cuda.synchronize()
+    assert (ref.e[:T] != mpf.EZ).any()
+    assert torch.equal(ref.m, got.m) and torch.equal(ref.e, got.e)
+    before = got.e.clone()
+    rc = lib.b3d_pole_level_noalloc(L, *args(T + 1, got), _p(got.m), _p(got.e), got.m.stride(0), stream)
+    assert rc == -2 and b"scratch" in lib.b3d_last_error()
+    torch.cuda.synchronize()
+    assert torch.equal(before, got.e)
