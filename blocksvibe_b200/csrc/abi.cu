@@ -109,6 +109,24 @@ int b3d_moments_level(int L, const int32_t* rm, const int64_t* re, int64_t rplan
                                            mplane, as_stream(stream)), "b3d_moments_level"));
 }
 
+int b3d_moments_stage(int L, const int32_t* rm, const int64_t* re, int64_t rplane, const int32_t* pm,
+                      const int64_t* pe, int64_t pplane, const int64_t* q_slot, const int64_t* q_row,
+                      const int64_t* q_n, int64_t Q, int64_t N, int64_t w, int64_t rows, int32_t* ym, int64_t* ye,
+                      int64_t yplane, void* stream) {
+    if (!nonneg(Q) || !nonneg(N) || !nonneg(w) || !nonneg(rows)) return fail(B3D_E_ARG, "b3d_moments_stage: invalid size");
+    B3D_DISPATCH(L, cuda_status(LX::moments_stage(rm, re, rplane, pm, pe, pplane, q_slot, q_row, q_n, Q, N, w, rows, ym,
+                                                 ye, yplane, as_stream(stream)), "b3d_moments_stage"));
+}
+
+int b3d_moments_flush(int L, const int32_t* ym, const int64_t* ye, int64_t yplane, const int64_t* row_shift, int64_t m0,
+                      int W, int64_t rows, int64_t N, int R1, const uint32_t* nk, const int32_t* nkb, int NN, int KW,
+                      int accumulate, int32_t* mm, int64_t* me, int64_t mplane, void* stream) {
+    if (!nonneg(rows) || !nonneg(N) || !nonneg(m0) || W < 0 || R1 < 1 || R1 > 32 || NN < 1 || KW < 1 || KW > 12)
+        return fail(B3D_E_ARG, "b3d_moments_flush: invalid size (1 <= R + 1 <= 32, 1 <= KW <= 12)");
+    B3D_DISPATCH(L, cuda_status(LX::moments_flush(ym, ye, yplane, row_shift, m0, W, rows, N, R1, nk, nkb, NN, KW,
+                                                 accumulate, mm, me, mplane, as_stream(stream)), "b3d_moments_flush"));
+}
+
 namespace {
 b3d::RnsTables tables_of(const b3d_rns_tables* t) {
     return b3d::RnsTables{t->p, t->mu, t->w, t->conv, t->inv, t->mj, t->mfull, t->rp, t->np, t->ml};

@@ -647,6 +647,145 @@ __global__ void __launch_bounds__(kMomThreads, 3) k_moments(const int32_t* __res
 }
 
 // ------------------------------------------------------------------------------------------------
+// Staged derivative moments.  Instead of a read-modify-write of all R + 1 moments of a row at every level,
+// each level only stages its terms, and the moments are formed once per window of levels:
+//   stage (per level m):  Y[m - m0, row, c] = round(res[slot, c] * rc^n)     (n = m + shift of the row's pole)
+//   flush (per window):   mom[row, kk, c] (+)= round( sum_{w < W} n_w^kk Y[w, row, c] ),  n_w = m0 + w + shift
+// The window sum is exact for every term above 2^-(32 L + 64) of the largest one (aligned to the largest
+// n^kk |Y| of the window, truncated below): one rounding per window and moment order, plus one for the
+// addition into the moments of earlier windows.  Staged entries that a level does not write stay zero.
+template <int L>
+__global__ void __launch_bounds__(kMomThreads, 3) k_moments_stage(const int32_t* __restrict__ rm, const i64* __restrict__ re,
+                          i64 rplane, const int32_t* __restrict__ pm, const i64* __restrict__ pe, i64 pplane,
+                          const i64* __restrict__ q_slot, const i64* __restrict__ q_row, const i64* __restrict__ q_n,
+                          i64 Q, i64 N, i64 w, i64 rows, int32_t* __restrict__ ym, i64* __restrict__ ye, i64 yplane) {
+    i64 t = blockIdx.x * (i64)blockDim.x + threadIdx.x;
+    if (t >= Q * N) return;
+    i64 c = t % N, q = t / N;
+    i64 ix = q_slot[q] * N + c, nn = q_n[q];
+    i64 out = (w * rows + q_row[q]) * N + c;
+    u32 x[L], p[L];
+    bool nx = load_mag<L>(rm, rplane, ix, x);
+    bool np = load_mag<L>(pm, pplane, nn, p);
+    i64 ex = re[ix], ep = pe[nn];
+    if (is_zero(x) || is_zero(p) || ex == EZ || ep == EZ) {
+        ye[out] = EZ;
+        return;
+    }
+    constexpr int NW = 2 * L + 1;
+    extern __shared__ u32 stage_acc[];                   // (NW, blockDim.x): this thread's product
+    u32* accm = stage_acc + threadIdx.x;
+#pragma unroll
+    for (int k = 0; k < NW; k++) accm[k * kMomThreads] = 0;
+    mac_signed_mem<L, NW>(accm, kMomThreads, x, p, false);
+    u32 acc[NW];
+#pragma unroll
+    for (int k = 0; k < NW; k++) acc[k] = accm[k * kMomThreads];
+    u32 y[L];
+    i64 ey;
+    round_mag<L>(acc, ex + ep, y, &ey);
+    store_signed<L>(ym, yplane, out, y, nx != np);
+    ye[out] = ey;
+}
+
+// One lane per moment order kk: a warp serves floor(32 / R1) (row, column) items, every lane of an item reading
+// the same staged numbers (broadcast loads) and forming its own order's exact window sum.  nk: n^kk as KW
+// little-endian 32-bit limbs, nk[(kk * NN + n) * KW + j]; nkb[kk * NN + n] its bit length (0 for 0^kk, kk > 0).
+template <int L, int KW>
+__global__ void __launch_bounds__(kMomThreads) k_moments_flush(const int32_t* __restrict__ ym, const i64* __restrict__ ye,
+                          i64 yplane, const i64* __restrict__ row_shift, i64 m0, int W, i64 rows, i64 N, int R1,
+                          const u32* __restrict__ nk, const int32_t* __restrict__ nkb, int NN, int accumulate,
+                          int32_t* __restrict__ mm, i64* __restrict__ me, i64 mplane) {
+    constexpr int NB = nb_bits(L);
+    constexpr int ACC = L + 3;                           // two's complement; magnitudes below 2^(32 (L + 2))
+    const int lane = threadIdx.x & 31, per = 32 / R1;
+    const int sub = lane / R1, kk = lane - sub * R1;
+    if (sub >= per) return;
+    const i64 item = ((blockIdx.x * (i64)blockDim.x + threadIdx.x) >> 5) * per + sub;
+    if (item >= rows * N) return;
+    const i64 row = item / N, c = item - row * N;
+    const i64 sh = row_shift[row];
+    i64 E = EZ;                                          // bound on the top bit of the window's terms
+    for (int w = 0; w < W; w++) {
+        const i64 ey = ye[(w * rows + row) * N + c];
+        const i64 n = m0 + w + sh;
+        if (ey == EZ || n >= NN) continue;
+        const int kb = nkb[kk * NN + n];
+        if (kb == 0) continue;
+        const i64 top = ey + NB + kb;
+        if (top > E) E = top;
+    }
+    const i64 o = (row * R1 + kk) * N + c;
+    if (E == EZ) {
+        if (!accumulate) {
+#pragma unroll
+            for (int k = 0; k < L; k++) mm[k * mplane + o] = 0;
+            me[o] = EZ;
+        }
+        return;
+    }
+    const i64 base = E - 32 * (L + 2);                   // weight of the accumulator's lowest bit
+    u32 acc[ACC];
+    zero(acc);
+    for (int w = 0; w < W; w++) {
+        const i64 ix = (w * rows + row) * N + c;
+        const i64 ey = ye[ix];
+        const i64 n = m0 + w + sh;
+        if (ey == EZ || n >= NN) continue;
+        if (nkb[kk * NN + n] == 0) continue;
+        u32 y[L];
+        const bool neg = load_mag<L>(ym, yplane, ix, y);
+        u32 P[L + KW];                                   // |Y| n^kk, exact
+        zero(P);
+#pragma unroll
+        for (int j = 0; j < KW; j++) {
+            const u32 b = nk[((i64)kk * NN + n) * KW + j];
+            u32 carry = 0;
+#pragma unroll
+            for (int i = 0; i < L; i++) {
+                const u64 v = (u64)y[i] * b + P[i + j] + carry;
+                P[i + j] = (u32)v;
+                carry = (u32)(v >> 32);
+            }
+#pragma unroll
+            for (int i = L + j; i < L + KW; i++) {
+                const u64 v = (u64)P[i] + carry;
+                P[i] = (u32)v;
+                carry = (u32)(v >> 32);
+            }
+        }
+        const i64 off = ey - base;                       // bit position of P's lowest bit in the accumulator
+        u32 T[ACC];
+        if (off >= 0) {
+            shl(P, (int)off, T);
+        } else if (-off < 32 * (L + KW)) {
+            shr(P, (int)(-off), T);
+        } else {
+            continue;
+        }
+        add_signed(acc, T, neg);
+    }
+    const bool neg = (acc[ACC - 1] >> 31) != 0;
+    if (neg) negate(acc);
+    u32 r[L];
+    i64 er;
+    bool nr = neg;
+    if (!round_mag<L>(acc, base, r, &er)) nr = false;
+    if (accumulate) {
+        u32 v[L], sum[L];
+        const bool nv = load_mag<L>(mm, mplane, o, v);
+        bool ns;
+        i64 es;
+        add_norm<L>(v, nv, me[o], r, nr, er, sum, &ns, &es);
+        store_signed<L>(mm, mplane, o, sum, ns);
+        me[o] = es;
+    } else {
+        store_signed<L>(mm, mplane, o, r, nr);
+        me[o] = er;
+    }
+}
+
+// ------------------------------------------------------------------------------------------------
 // Host-side launchers, one instantiation per limb count (inst.cu).  Each returns a cudaError_t code.
 inline unsigned grid_for(i64 n, int th) { return (unsigned)((n + th - 1) / th); }
 
@@ -673,6 +812,12 @@ struct Launch {
     static int moments(const int32_t* rm, const i64* re, i64 rplane, const int32_t* pm, const i64* pe, i64 pplane,
                        const i64* q_slot, const i64* q_row, const i64* q_n, i64 Q, i64 N, int R1,
                        int32_t* mm, i64* me, i64 mplane, cudaStream_t st);
+    static int moments_stage(const int32_t* rm, const i64* re, i64 rplane, const int32_t* pm, const i64* pe, i64 pplane,
+                             const i64* q_slot, const i64* q_row, const i64* q_n, i64 Q, i64 N, i64 w, i64 rows,
+                             int32_t* ym, i64* ye, i64 yplane, cudaStream_t st);
+    static int moments_flush(const int32_t* ym, const i64* ye, i64 yplane, const i64* row_shift, i64 m0, int W, i64 rows,
+                             i64 N, int R1, const u32* nk, const int32_t* nkb, int NN, int KW, int accumulate,
+                             int32_t* mm, i64* me, i64 mplane, cudaStream_t st);
 };
 
 #ifdef B3D_DEFINE_LAUNCH
@@ -771,6 +916,35 @@ int Launch<L>::moments(const int32_t* rm, const i64* re, i64 rplane, const int32
     if (n == 0) return 0;
     k_moments<L><<<grid_for(n, kMomThreads), kMomThreads, (2 * L + 1) * kMomThreads * 4, st>>>(
         rm, re, rplane, pm, pe, pplane, q_slot, q_row, q_n, Q, N, R1, mm, me, mplane);
+    return (int)cudaGetLastError();
+}
+
+template <int L>
+int Launch<L>::moments_stage(const int32_t* rm, const i64* re, i64 rplane, const int32_t* pm, const i64* pe, i64 pplane,
+                             const i64* q_slot, const i64* q_row, const i64* q_n, i64 Q, i64 N, i64 w, i64 rows,
+                             int32_t* ym, i64* ye, i64 yplane, cudaStream_t st) {
+    i64 n = Q * N;
+    if (n == 0) return 0;
+    k_moments_stage<L><<<grid_for(n, kMomThreads), kMomThreads, (2 * L + 1) * kMomThreads * 4, st>>>(
+        rm, re, rplane, pm, pe, pplane, q_slot, q_row, q_n, Q, N, w, rows, ym, ye, yplane);
+    return (int)cudaGetLastError();
+}
+
+template <int L>
+int Launch<L>::moments_flush(const int32_t* ym, const i64* ye, i64 yplane, const i64* row_shift, i64 m0, int W, i64 rows,
+                             i64 N, int R1, const u32* nk, const int32_t* nkb, int NN, int KW, int accumulate,
+                             int32_t* mm, i64* me, i64 mplane, cudaStream_t st) {
+    const i64 items = rows * N;
+    if (items == 0 || W == 0) return 0;
+    const int per = 32 / R1;
+    const i64 warps = (items + per - 1) / per;
+    const unsigned grid = (unsigned)((warps * 32 + kMomThreads - 1) / kMomThreads);
+#define B3D_FLUSH(KWC) k_moments_flush<L, KWC><<<grid, kMomThreads, 0, st>>>(ym, ye, yplane, row_shift, m0, W, rows, N, R1, \
+                                                                         nk, nkb, NN, accumulate, mm, me, mplane)
+    if (KW <= 2) B3D_FLUSH(2);
+    else if (KW <= 6) B3D_FLUSH(6);
+    else B3D_FLUSH(12);
+#undef B3D_FLUSH
     return (int)cudaGetLastError();
 }
 #endif

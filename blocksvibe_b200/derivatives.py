@@ -31,6 +31,12 @@ from . import _lib, mpf, structure as S
 from .mpf import MPF
 
 
+# Moments: "staged" (each level stages its terms, exact window sums flushed once per window: b3d_moments_stage /
+# b3d_moments_flush) or "per_level" (read-modify-write of every moment at every level: b3d_moments_level).
+MOMENTS = "staged"
+STAGE_BYTES = 4 << 30           # device bytes of the staging window (whole levels; at least one)
+
+
 # ---------------------------------------------------------------- numerator basis (exact rationals)
 
 def _poly_from_roots(roots):
@@ -101,6 +107,10 @@ def to_x(poly_y, scale):
     return [v * Fraction(2) ** (k - scale) for k, v in enumerate(poly_y)]
 
 
+# per-run attributes (set by start / accumulate / flush): never shared through the for_order constants
+_RUN_STATE = ("B", "N", "mom", "_stage", "_staged_mode", "_W", "_m0", "_last", "_flushes")
+
+
 class Derivs:
     """Post-recursion stages for one Plan and any batch of right-hand sides with lambda orders
     n >= Lambda - R.  two_js: internal spins to output (default: all two_j <= two_j_max)."""
@@ -129,6 +139,10 @@ class Derivs:
         of task (p, tj, pole) at level m feeds moment row (p Jo + jo) NP + i (i: the pole's index in the block at
         full order) with weight n^k r_c^n, n = m + shift(pole)"""
         pl, Jo, NP, dev = self.plan, self.Jo, self.NP, self.device
+        shift = np.zeros((2, Jo, NP), dtype=np.int64)              # level shift of each row's pole
+        for jo, poles in enumerate(self.poles):
+            shift[:, jo, :len(poles)] = [S.level_shift(P) for P in poles]
+        self._row_shift = torch.as_tensor(shift.reshape(-1), device=dev)
         jo_of = np.full(pl.tjmax + 2 * pl.order + 3, -1, dtype=np.int64)
         jo_of[np.array(self.tjs, dtype=np.int64)] = np.arange(Jo)
         self.levels = []
@@ -168,12 +182,32 @@ class Derivs:
                     T[e][k] = (T[e - 1][k - 1] if k else 0) + D * T[e - 1][k]
             tables.append([x for row in T for x in row])
         self.Ttab = mpf.from_fractions([x for t in tables for x in t], L, (len(tables), R + 1, R + 1), dev)
+        self._power_tables()
         didx = np.zeros((Jo, NP), dtype=np.int64)
         for jo, t in enumerate(twice):
             didx[jo, :len(t)] = np.searchsorted(positions, t) + 1
         self.didx = torch.as_tensor(didx, device=dev)
         self._small_constants()
         self.Anum = self._numerator_matrix()
+
+    def _power_tables(self):
+        """n^k (k <= R, n <= order) as KW 32-bit limbs and their bit lengths, for the staged moments' flush"""
+        R1, NN = self.R + 1, self.plan.order + 1
+        need = max(1, -(-(max(n ** k for k in range(R1) for n in range(NN))).bit_length() // 32))
+        KW = next((w for w in (2, 6, 12) if w >= need), None)
+        if KW is None:
+            raise ValueError(f"n^k up to {self.plan.order}^{self.R} exceeds the flush kernel's 12 limbs")
+        limbs = np.zeros((R1, NN, KW), dtype=np.uint32)
+        bits = np.zeros((R1, NN), dtype=np.int32)
+        for k in range(R1):
+            for n in range(NN):
+                v = n ** k                                   # 0^0 = 1
+                bits[k, n] = v.bit_length()
+                for j in range(KW):
+                    limbs[k, n, j] = (v >> (32 * j)) & 0xFFFFFFFF
+        self._nk = torch.as_tensor(limbs.view(np.int32), device=self.device)
+        self._nkb = torch.as_tensor(bits, device=self.device)
+        self._KW = KW
 
     def _numerator_matrix(self):
         """A (Jo, Dout, NP + R + 1): per spin, the numerator basis (numerator_basis_y) in x, pole columns first
@@ -215,7 +249,7 @@ class Derivs:
         base = self._orders.get(R)
         if base is None:
             base = object.__new__(Derivs)
-            base.__dict__.update(self.__dict__)
+            base.__dict__.update({k: v for k, v in self.__dict__.items() if k not in _RUN_STATE})
             base.R, base.Dout = R, self.NPout + R + 1
             R1, K = R + 1, self.NP + R + 1
             base.Anum = MPF(self.Anum.m[:, :, :base.Dout, :K], self.Anum.e[:, :base.Dout, :K]).contiguous()
@@ -228,27 +262,68 @@ class Derivs:
         d.__dict__.update(base.__dict__)
         return d
 
+    def stage_window(self, B):
+        """levels per staging window for B right-hand sides (the whole order when it fits STAGE_BYTES)"""
+        per_level = (4 * self.L + 8) * 2 * self.Jo * self.NP * self.plan.Smax ** 2 * B
+        return int(max(1, min(self.plan.order, STAGE_BYTES // max(per_level, 1))))
+
     def footprint_bytes(self, B):
-        """device bytes of the moment accumulators for B right-hand sides"""
-        return (4 * self.L + 8) * 2 * self.Jo * self.NP * (self.R + 1) * self.plan.Smax ** 2 * B
+        """device bytes of the moment accumulators (and the staging window) for B right-hand sides"""
+        per = (4 * self.L + 8) * 2 * self.Jo * self.NP * self.plan.Smax ** 2 * B
+        return per * (self.R + 1 + (self.stage_window(B) if MOMENTS == "staged" else 0))
 
     # ------------------------------------------------------------ accumulation during the recursion
     def start(self, B):
         """zero moment accumulators (rows, R + 1, S^2 B) for a batch of B right-hand sides"""
         self.B = B
         self.N = self.plan.Smax ** 2 * B
-        self.mom = mpf.zeros((2 * self.Jo * self.NP, self.R + 1, self.N), self.L, self.device)
+        rows = 2 * self.Jo * self.NP
+        self.mom = mpf.zeros((rows, self.R + 1, self.N), self.L, self.device)
+        self._staged_mode = MOMENTS == "staged"
+        if self._staged_mode:
+            self._W = self.stage_window(B)
+            self._stage = mpf.zeros((self._W, rows, self.N), self.L, self.device)
+            self._m0, self._last, self._flushes = 0, None, 0
 
     def accumulate(self, m, res):
-        """recursion hook: add level m's residues of the output spins to the moments"""
+        """recursion hook: add level m's residues of the output spins to the moments (staged: into the window,
+        flushed into the moments when the window is full)"""
         lev = self.levels[m]
         if lev is None:
             return
         sl, rw, nn = lev
         p = lambda t: t.data_ptr()
-        _lib.call("b3d_moments_level", self.L, p(res.m), p(res.e), res.m.stride(0), p(self.rcpow.m), p(self.rcpow.e),
-                  self.rcpow.m.stride(0), p(sl), p(rw), p(nn), sl.numel(), self.N, self.R + 1,
-                  p(self.mom.m), p(self.mom.e), self.mom.m.stride(0), torch.cuda.current_stream(self.device).cuda_stream)
+        stream = torch.cuda.current_stream(self.device).cuda_stream
+        if not self._staged_mode:
+            _lib.call("b3d_moments_level", self.L, p(res.m), p(res.e), res.m.stride(0), p(self.rcpow.m), p(self.rcpow.e),
+                      self.rcpow.m.stride(0), p(sl), p(rw), p(nn), sl.numel(), self.N, self.R + 1,
+                      p(self.mom.m), p(self.mom.e), self.mom.m.stride(0), stream)
+            return
+        if m - self._m0 >= self._W:
+            self.flush()
+            self._m0 = m
+        rows = 2 * self.Jo * self.NP
+        _lib.call("b3d_moments_stage", self.L, p(res.m), p(res.e), res.m.stride(0), p(self.rcpow.m), p(self.rcpow.e),
+                  self.rcpow.m.stride(0), p(sl), p(rw), p(nn), sl.numel(), self.N, m - self._m0, rows,
+                  p(self._stage.m), p(self._stage.e), self._stage.m.stride(0), stream)
+        self._last = m
+
+    def flush(self):
+        """form the moments of the staged window (no-op without staged levels); the window is then empty"""
+        if not getattr(self, "_staged_mode", False) or self._last is None:
+            return
+        p = lambda t: t.data_ptr()
+        rows, W = 2 * self.Jo * self.NP, self._last - self._m0 + 1
+        R1 = self.R + 1
+        nk = self._nk[:R1].contiguous()
+        nkb = self._nkb[:R1].contiguous()
+        _lib.call("b3d_moments_flush", self.L, p(self._stage.m), p(self._stage.e), self._stage.m.stride(0),
+                  p(self._row_shift), self._m0, W, rows, self.N, R1, p(nk), p(nkb), self.plan.order + 1, self._KW,
+                  int(self._flushes > 0), p(self.mom.m), p(self.mom.e), self.mom.m.stride(0),
+                  torch.cuda.current_stream(self.device).cuda_stream)
+        self._flushes += 1
+        self._last = None
+        self._stage.e.fill_(mpf.EZ)                      # entries a level does not write read as zero
 
     # ------------------------------------------------------------ final GEMMs
     def finish(self, h_inf, chunk=None):
@@ -258,6 +333,7 @@ class Derivs:
 
     def finish_iter(self, h_inf, chunk=None):
         """as finish, by chunks of output spins: yields (first spin index, numerators)"""
+        self.flush()
         R, Jo, NP, order, L, dev = self.R, self.Jo, self.NP, self.plan.order, self.L, self.device
         R1, N, Rw = R + 1, self.N, max(R, 1)
         S2 = self.plan.Smax ** 2

@@ -144,6 +144,7 @@ class Operator:
         d = self.der.for_order(self.der.R)                 # own accumulators: concurrent batches may share self
         d.start(nq * no)
         self.rec.run(h, hook=d.accumulate)
+        d.flush()
         S2 = self.plan.Smax ** 2
         mom = d.mom.reshape(d.mom.shape[0], d.R + 1, S2, nq, no)
         nums = []

@@ -99,6 +99,23 @@ int b3d_moments_level(int L, const int32_t* rm, const int64_t* re, int64_t rplan
                       const int64_t* q_n, int64_t Q, int64_t N, int R1, int32_t* mm, int64_t* me, int64_t mplane,
                       void* stream);
 
+/* Staged derivative moments (replaces the per-level momacc and the windowed momflush + mpadd of the reference,
+ * derivatives.py:48-188, :474-510).  Stage, once per level m of a window starting at m0 (w = m - m0): for each
+ * entry q and column c, Y[(w * rows + q_row[q]) * N + c] = res[q_slot[q], c] * rcpow[q_n[q]] (one rounding);
+ * Y exponents the level does not write must be B3D_EZ (the caller clears them per window). */
+int b3d_moments_stage(int L, const int32_t* rm, const int64_t* re, int64_t rplane, const int32_t* pm,
+                      const int64_t* pe, int64_t pplane, const int64_t* q_slot, const int64_t* q_row,
+                      const int64_t* q_n, int64_t Q, int64_t N, int64_t w, int64_t rows, int32_t* ym, int64_t* ye,
+                      int64_t yplane, void* stream);
+
+/* Flush a window of W staged levels: mom[(row * R1 + k) * N + c] = (mom +) round(sum_w n^k Y[w, row, c]) with
+ * n = m0 + w + row_shift[row] (< NN), the sum exact above 2^-(32 L + 64) of its largest term, one rounding (and one
+ * for the addition when accumulate != 0).  nk: n^k as KW 32-bit limbs, nk[(k * NN + n) * KW + j]; nkb[k * NN + n]
+ * its bit length.  R1 <= 32, KW <= 12. */
+int b3d_moments_flush(int L, const int32_t* ym, const int64_t* ye, int64_t yplane, const int64_t* row_shift, int64_t m0,
+                      int W, int64_t rows, int64_t N, int R1, const uint32_t* nk, const int32_t* nkb, int NN, int KW,
+                      int accumulate, int32_t* mm, int64_t* me, int64_t mplane, void* stream);
+
 /* ---- residue-number-system GEMM on the INT8 tensor cores (tcgen05), the replacement of the reference's
  * un-vendored sdpvibe mpf.gemm (RNS / INT8; called at recursion_gpu.py:53-79, derivatives.py:540-580,
  * output.py:189,211).  Exact products, one rounding: bit-identical to b3d_gemm_aligned. */

@@ -71,6 +71,54 @@ def test_pole_shifted_numerators_match_oracle(cuda, case, R, kept):
     compare_numerators(case, M, H, plan, der, num, R, kept=kept)
 
 
+@pytest.mark.parametrize("mode,stage_bytes", [("staged", 1 << 40), ("staged", 1), ("per_level", 1 << 40)])
+def test_moment_modes_match_oracle(cuda, mode, stage_bytes, monkeypatch):
+    """the staged moments with one window for the whole recursion, with a one-level window (a flush and an
+    addition into the moments at every level), and the per-level read-modify-write: numerators against the oracle"""
+    monkeypatch.setattr(DV, "MOMENTS", mode)
+    monkeypatch.setattr(DV, "STAGE_BYTES", stage_bytes)
+    case, R, kept = (4, 2, 6, 9, ((0, 1), (1, 0)), 10, 2, 61), 4, 6
+    M, H, plan, der, num = run_numerators(case, cuda, R, kept=kept)
+    compare_numerators(case, M, H, plan, der, num, R, kept=kept)
+
+
+def test_staged_window_sums_cancel_exactly(cuda, monkeypatch):
+    """the flush's window sum is exact: staged terms y = (x, -2 x, x) at n = (s, s + 1, s + 2) (a second difference)
+    give exact zeros for the moments of order 0 and 1 and the correctly rounded sum for the higher orders"""
+    L, order, R = 10, 6, 3
+    plan = PL.Plan(0, 0, 2, order, ((0, 0), (1, 1)), reuse=True)
+    der = DV.Derivs(plan, R, L, device=cuda)
+    rows, N = 2 * der.Jo * der.NP, 3
+    W = 3
+    with mp.workprec(32 * L + 64):
+        x = mp.mpf(3) / 7
+        s = int(der._row_shift[0])                       # row 0's pole: n = w + s at window level w
+        n = [w + s for w in range(W)]
+        y = [x, -2 * x, x]
+        vals = []
+        for w in range(W):
+            for r in range(rows):
+                for c in range(N):
+                    vals.append(y[w] if r == 0 else mp.mpf(0))
+    stage = mpf.from_mp(vals, L, (W, rows, N), cuda)
+    mom = mpf.zeros((rows, R + 1, N), L, cuda)
+    p = lambda t: t.data_ptr()
+    from blocksvibe_b200 import _lib
+    _lib.call("b3d_moments_flush", L, p(stage.m), p(stage.e), stage.m.stride(0), p(der._row_shift), 0, W, rows, N, R + 1,
+              p(der._nk[:R + 1].contiguous()), p(der._nkb[:R + 1].contiguous()), order + 1, der._KW, 0, p(mom.m),
+              p(mom.e), mom.m.stride(0), torch.cuda.current_stream(cuda).cuda_stream)
+    got = mpf.to_mp(mom)
+    with mp.workprec(32 * L + 200):
+        for k in range(R + 1):
+            want = mp.fsum(mp.mpf(nn) ** k * yy for nn, yy in zip(n, y))
+            for c in range(N):
+                if want == 0:
+                    assert got[0, k, c] == 0
+                else:
+                    assert abs(got[0, k, c] - want) <= abs(want) * mp.mpf(2) ** (2 - (32 * L - 2))
+        assert all(v == 0 for v in got[1:].reshape(-1))
+
+
 def test_for_order_views(cuda):
     """Derivs.for_order(R') (a higher lambda order) gives the numerators of a Derivs built for R'"""
     case = (2, 2, 4, 7, ((0, 0), (1, 1)), 10, 1, 51)

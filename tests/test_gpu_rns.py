@@ -85,3 +85,38 @@ def test_autotuned_gemm_equals_schoolbook(cuda):
                 assert torch.equal(ref.m, got.m) and torch.equal(ref.e, got.e)
     finally:
         mpf.GEMM_BACKEND, mpf.AUTOTUNE = "auto", False
+
+
+def _extreme(shape, L, neg, device):
+    """MPF of the largest NB-bit magnitude, 2^NB - 1, exponent 0, sign neg (a bool tensor of the shape)"""
+    NB = 32 * L - 2
+    v = (1 << NB) - 1
+    pos = [(v >> (32 * k)) & 0xFFFFFFFF for k in range(L)]
+    negl = [((1 << (32 * L)) - v >> (32 * k)) & 0xFFFFFFFF for k in range(L)]
+    m = torch.empty((L,) + tuple(shape), dtype=torch.int64)
+    for k in range(L):
+        m[k] = torch.where(neg, negl[k], pos[k])
+    m = ((m + (1 << 31)) % (1 << 32) - (1 << 31)).to(torch.int32)
+    return mpf.MPF(m.to(device), torch.zeros(shape, dtype=torch.int64, device=device))
+
+
+@pytest.mark.parametrize("L", [10, 34, 42])
+@pytest.mark.parametrize("signs", ["positive", "negative", "alternating"])
+@pytest.mark.parametrize("crt", ["tensor", "cuda"])
+def test_rns_gemm_largest_products(cuda, L, signs, crt):
+    """the largest products the residue GEMM meets: K = 256 terms of two all-ones NB-bit magnitudes, all of one
+    sign (|P| = 256 (2^NB - 1)^2, x' far from its reduced value) or alternating; bitwise the schoolbook GEMM"""
+    M_, K, N = 6, 256, 9
+    if signs == "alternating":
+        na = (torch.arange(M_ * K).reshape(1, M_, K) % 2) == 1
+        nb = torch.zeros((1, K, N), dtype=torch.bool)
+    else:
+        na = torch.full((1, M_, K), signs == "negative")
+        nb = torch.zeros((1, K, N), dtype=torch.bool)
+    A, B = _extreme((1, M_, K), L, na, cuda), _extreme((1, K, N), L, nb, cuda)
+    Aal, Bal = mpf.align_rows(A), mpf.align_cols(B)
+    ref = mpf.gemm_aligned(Aal, Bal)
+    got = rns.gemm_aligned_rns(Aal, Bal, crt=crt)
+    torch.cuda.synchronize()
+    rns.check_errors(cuda)
+    assert torch.equal(ref.e, got.e) and torch.equal(ref.m, got.m)
