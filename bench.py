@@ -44,6 +44,8 @@ def parse():
     ap.add_argument("--no-graph", action="store_true", help="launch every kernel from Python instead of a CUDA graph")
     ap.add_argument("--rate", type=float, default=200.0, help="cfg4: Poisson arrival rate (tasks/s)")
     ap.add_argument("--requests", type=int, default=32, help="cfg4: requests in the stream")
+    ap.add_argument("--cauchy", default=None, help="Cauchy kernel form (Recursion's cauchy argument)")
+    ap.add_argument("--moments", default=None, choices=(None, "staged", "per_level"), help="moments form")
     ap.add_argument("--no-set644", action="store_true", help="default run: skip the full 644-task set")
     ap.add_argument("--no-cfg4", action="store_true", help="default run: skip the serving stream at its stated rate")
     return ap.parse_args()
@@ -146,7 +148,7 @@ class Clocks:
 
 
 # ---------------------------------------------------------------- kernel probe (launch count, per-kernel events)
-KERNELS_PER_CALL = {"b3d_pole_level": 2, "b3d_cauchy_align": 2}
+KERNELS_PER_CALL = {"b3d_pole_level": 2, "b3d_cauchy_align": 2, "b3d_cauchy_align_sm": 2}
 
 
 class Probe:
@@ -471,7 +473,7 @@ def run_ours(args):
     # roofline of the dominant kernel: algorithmic bytes per launch / mean launch time
     L, N, S = op.L, op.plan.Smax ** 2 * (len(ns) if args.schedule == "batched" else 1), op.plan.Smax
     levs = [lv for lv in op.plan.levels if lv]
-    if dominant in ("b3d_cauchy_level", "b3d_cauchy_level2", "b3d_cauchy_level3"):
+    if dominant in ("b3d_cauchy_level", "b3d_cauchy_level2", "b3d_cauchy_level3", "b3d_cauchy_level4"):
         per_step_bytes = sum(RL.cauchy_level_bytes(lv, N, L) for lv in levs if lv["m"] > 0 or dominant == "b3d_cauchy_level") \
             * (1 if args.schedule == "batched" else len(ns))
     elif dominant == "b3d_pole_level":
@@ -744,6 +746,11 @@ def run_stream(args):
 
 def main():
     args = parse()
+    from blocksvibe_b200 import derivatives as DV, recursion as RC
+    if args.cauchy:
+        RC.CAUCHY = args.cauchy
+    if args.moments:
+        DV.MOMENTS = args.moments
     if args.impl == "reference":
         run_reference(args)
     elif args.workload == "set644":

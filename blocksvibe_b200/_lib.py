@@ -26,6 +26,8 @@ SIGNATURES = {
     "b3d_cauchy_align": [_I, _P, _P, _Q, _P, _P, _P, _Q, _P],
     "b3d_cauchy_level2": [_I, _P, _P, _Q, _P, _P, _Q, _P, _P, _P, _Q, _P],
     "b3d_cauchy_level3": [_I, _P, _P, _Q, _P, _P, _Q, _P, _Q, _P, _P, _Q, _P],
+    "b3d_cauchy_align_sm": [_I, _P, _P, _Q, _P, _P, _P, _Q, _P],
+    "b3d_cauchy_level4": [_I, _P, _P, _Q, _P, _P, _Q, _P, _Q, _P, _P, _Q, _P],
     "b3d_cauchy_digits": [_P, _P, _Q, _I, _Q, _Q, _I, _Q, _P, _P],
     "b3d_cauchy_add_hinf": [_I, _P, _P, _Q, _P, _P, _Q, _P, _P, _P, _Q, _P],
     "b3d_pole_level_noalloc": [_I, _P, _P, _Q, _P, _P, _Q, _P, _P, _Q, _P, _P, _P, _P, _Q, _Q, _I, _P, _P, _Q, _P],
@@ -61,6 +63,8 @@ SIGNATURES["b3d_cauchy_align"][4] = ctypes.POINTER(LevelTables)
 SIGNATURES["b3d_cauchy_digits"][0] = ctypes.POINTER(LevelTables)
 SIGNATURES["b3d_cauchy_level2"][7] = ctypes.POINTER(LevelTables)
 SIGNATURES["b3d_cauchy_level3"][7] = ctypes.POINTER(LevelTables)
+SIGNATURES["b3d_cauchy_align_sm"][4] = ctypes.POINTER(LevelTables)
+SIGNATURES["b3d_cauchy_level4"][7] = ctypes.POINTER(LevelTables)
 SIGNATURES["b3d_cauchy_add_hinf"][7] = ctypes.POINTER(LevelTables)
 ctypes_byref = ctypes.byref
 

@@ -214,6 +214,26 @@ int b3d_cauchy_align(int L, const int32_t* rm, const int64_t* re, int64_t rplane
     B3D_DISPATCH_CAUCHY(L, cuda_status(CX::align(rm, re, rplane, c, om, oe, oplane, as_stream(stream)), "b3d_cauchy_align"));
 }
 
+int b3d_cauchy_align_sm(int L, const int32_t* rm, const int64_t* re, int64_t rplane, const b3d_level_tables* lv,
+                        int32_t* om, int64_t* oe, int64_t oplane, void* stream) {
+    if (!level_ok(lv)) return fail(B3D_E_ARG, "b3d_cauchy_align_sm: invalid level description");
+    b3d::CauchyLevel c = level_of(lv);
+    B3D_DISPATCH_CAUCHY(L, cuda_status(CX::align_sm(rm, re, rplane, c, om, oe, oplane, as_stream(stream)),
+                                       "b3d_cauchy_align_sm"));
+}
+
+int b3d_cauchy_level4(int L, const int32_t* xm, const int64_t* xe, int64_t xplane, const int32_t* hm,
+                      const int64_t* he, int64_t hplane, const b3d_level_tables* lv, int64_t dmax, int32_t* om,
+                      int64_t* oe, int64_t oplane, void* stream) {
+    if (!level_ok(lv)) return fail(B3D_E_ARG, "b3d_cauchy_level4: invalid level description");
+    if (dmax < 1 || dmax >= (1 << 16)) return fail(B3D_E_ARG, "b3d_cauchy_level4: dmax must be in [1, 65535]");
+    if (dmax >= (1 << 10) && lv->Kc >= 2048)
+        return fail(B3D_E_ARG, "b3d_cauchy_level4: more than 2047 columns with 16-bit digits");
+    b3d::CauchyLevel c = level_of(lv);
+    B3D_DISPATCH(L, cuda_status(LX::cauchy4(xm, xe, xplane, hm, he, hplane, c, dmax, om, oe, oplane, as_stream(stream)),
+                                "b3d_cauchy_level4"));
+}
+
 int b3d_cauchy_level2(int L, const int32_t* xm, const int64_t* xe, int64_t xplane, const int32_t* hm,
                       const int64_t* he, int64_t hplane, const b3d_level_tables* lv, int32_t* om, int64_t* oe,
                       int64_t oplane, void* stream) {

@@ -53,6 +53,31 @@ __global__ void k_cauchy_align(const int32_t* __restrict__ rm, const i64* __rest
     store_signed<L>(om, oplane, t, s, neg);
 }
 
+// k_cauchy_align with sign-magnitude output: |x| aligned, the sign in bit 31 of limb L - 1 (free: |x| < 2^NB),
+// the input form of k_cauchy4
+template <int L>
+__global__ void k_cauchy_align_sm(const int32_t* __restrict__ rm, const i64* __restrict__ re, i64 rplane, CauchyLevel lv,
+                                  const i64* __restrict__ ce, int32_t* __restrict__ om, i64 oplane) {
+    i64 t = blockIdx.x * (i64)blockDim.x + threadIdx.x;
+    const i64 N = lv.N;
+    if (t >= lv.nb * lv.Kc * N) return;
+    const i64 n = t % N, i = (t / N) % lv.Kc, g = t / (N * lv.Kc);
+    const i64 E = ce[g * N + n];
+    u32 a[L], s[L];
+    bool neg = false;
+    if (i < lv.ncol[g] && E != EZ) {
+        const i64 ix = lv.col[g * lv.Kc + i] * N + n;
+        neg = load_mag<L>(rm, rplane, ix, a);
+        const i64 ei = re[ix];
+        if (is_zero(a) || ei == EZ || E - ei >= 32 * L) { zero(s); neg = false; }
+        else shr(a, (int)(E - ei), s);
+    } else {
+        zero(s);
+    }
+#pragma unroll
+    for (int k = 0; k < L; k++) om[k * oplane + t] = (int32_t)(k == L - 1 && neg ? (s[k] | 0x80000000u) : s[k]);
+}
+
 #ifdef B3D_RNS_MMA
 // digit matrices of C: matrix (prime j, group g), rows 4 r + s, columns i, tiles of TR digit rows; threads over
 // (g, r < Rp, i4 < Kp / 4), four consecutive i per thread.  table[(d + dmax) * np + j] = residue of
@@ -122,6 +147,8 @@ struct CauchyRnsLaunch {
                      i64 oplane, cudaStream_t st);
     static int add_hinf(const int32_t* am, const i64* ae, i64 aplane, const int32_t* hm, const i64* he, i64 hplane,
                         const CauchyLevel& lv, int32_t* om, i64* oe, i64 oplane, cudaStream_t st);
+    static int align_sm(const int32_t* rm, const i64* re, i64 rplane, const CauchyLevel& lv, int32_t* om, i64* oe,
+                        i64 oplane, cudaStream_t st);
 };
 
 #ifdef B3D_DEFINE_LAUNCH
@@ -132,6 +159,16 @@ int CauchyRnsLaunch<L>::align(const int32_t* rm, const i64* re, i64 rplane, cons
     if (n == 0) return 0;
     k_cauchy_colexp<L><<<(unsigned)((n + 127) / 128), 128, 0, st>>>(rm, re, rplane, lv, oe);
     if (ne > 0) k_cauchy_align<L><<<(unsigned)((ne + 127) / 128), 128, 0, st>>>(rm, re, rplane, lv, oe, om, oplane);
+    return (int)cudaGetLastError();
+}
+
+template <int L>
+int CauchyRnsLaunch<L>::align_sm(const int32_t* rm, const i64* re, i64 rplane, const CauchyLevel& lv, int32_t* om,
+                                 i64* oe, i64 oplane, cudaStream_t st) {
+    const i64 n = lv.nb * lv.N, ne = n * lv.Kc;
+    if (n == 0) return 0;
+    k_cauchy_colexp<L><<<(unsigned)((n + 127) / 128), 128, 0, st>>>(rm, re, rplane, lv, oe);
+    if (ne > 0) k_cauchy_align_sm<L><<<(unsigned)((ne + 127) / 128), 128, 0, st>>>(rm, re, rplane, lv, oe, om, oplane);
     return (int)cudaGetLastError();
 }
 

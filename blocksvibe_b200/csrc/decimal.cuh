@@ -295,46 +295,98 @@ template <int L> __device__ __forceinline__ bool less_norm(i64 ea, const u32 (&a
 }
 
 // kept size of each polynomial (0: all zero) and the byte length of its text (-1 when a kept coefficient is
-// outside the formatter's range; dropped coefficients may be)
+// outside the formatter's range; dropped coefficients may be).  blocks_3d's rule, scanning from the top
+// coefficient down, keeps the polynomial up to the lowest nonzero coefficient c_d whose higher coefficients are
+// all below eps |c_d|:  size = 1 + min { d : c_d != 0 and max_{d' > d} |c_d'| < eps |c_d| }.  One warp per
+// polynomial, one coefficient per lane (coalesced loads of the limb planes): chunks of 32 coefficients from the
+// top, an exact suffix maximum of the normalised magnitudes by shuffles, carried from chunk to chunk.
 template <int L>
 __global__ void k_poly_sizes(const int32_t* __restrict__ m, const i64* __restrict__ e, i64 plane,
                              const i64* __restrict__ poly_num, i64 npoly, int D, int eps_shift,
                              const int32_t* __restrict__ len, int32_t* __restrict__ size, i64* __restrict__ text_len) {
-    const i64 t = blockIdx.x * (i64)blockDim.x + threadIdx.x;
-    if (t >= npoly) return;
+    const i64 t = (blockIdx.x * (i64)blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (t >= npoly) return;                                  // whole warps leave together
     const i64 base = poly_num[t];
-    u32 mx[L];
-    zero(mx);
-    i64 emx = 0;
-    bool mxz = true, any = false;
-    int sz = D;
-    for (int d = D - 1; d >= 0; d--) {
+    // carried maximum of the coefficients above the current chunk (ce == EZ: none yet)
+    u32 cm[L];
+    zero(cm);
+    i64 ce = EZ;
+    int sz = -1;                                             // lowest d with the condition (-1: none yet)
+    for (int top = D - 1; top >= 0; top -= 32) {
+        const int d = top - lane;                            // lane 0: the highest coefficient of the chunk
         u32 c[L];
-        load_mag<L>(m, plane, base + d, c);
-        const i64 ec = e[base + d];
-        if (ec == EZ || is_zero(c)) continue;               // |c| = 0: neither condition holds
-        any = true;
-        const i64 en = ec - normalise(c);
-        if (mxz || less_norm<L>(emx, mx, en - eps_shift, c)) sz = d + 1;
-        if (mxz || less_norm<L>(emx, mx, en, c)) {
+        zero(c);
+        i64 en = EZ;
+        if (d >= 0) {
+            load_mag<L>(m, plane, base + d, c);
+            const i64 ec = e[base + d];
+            if (ec != EZ && !is_zero(c)) en = ec - normalise(c);
+            else zero(c);
+        }
+        // exclusive prefix maximum over lanes 0 .. lane - 1 (the higher coefficients of the chunk), then the carry
+        u32 mx[L];
+        i64 emx = EZ;
+        {
+            u32 run[L];
+            i64 erun = en;
 #pragma unroll
-            for (int k = 0; k < L; k++) mx[k] = c[k];
-            emx = en;
-            mxz = false;
+            for (int k = 0; k < L; k++) run[k] = c[k];
+#pragma unroll
+            for (int off = 1; off < 32; off <<= 1) {         // inclusive scan of the maximum towards higher lanes
+                u32 o[L];
+#pragma unroll
+                for (int k = 0; k < L; k++) o[k] = __shfl_up_sync(0xFFFFFFFFu, run[k], off);
+                const i64 eo = __shfl_up_sync(0xFFFFFFFFu, erun, off);
+                if (lane >= off && eo != EZ && (erun == EZ || less_norm<L>(erun, run, eo, o))) {
+#pragma unroll
+                    for (int k = 0; k < L; k++) run[k] = o[k];
+                    erun = eo;
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < L; k++) mx[k] = __shfl_up_sync(0xFFFFFFFFu, run[k], 1);
+            emx = __shfl_up_sync(0xFFFFFFFFu, erun, 1);
+            if (lane == 0) emx = EZ;
+            if (ce != EZ && (emx == EZ || less_norm<L>(emx, mx, ce, cm))) {
+#pragma unroll
+                for (int k = 0; k < L; k++) mx[k] = cm[k];
+                emx = ce;
+            }
+            // the new carry: the maximum of the whole chunk and the old carry (lane 31's inclusive value)
+            u32 last[L];
+#pragma unroll
+            for (int k = 0; k < L; k++) last[k] = __shfl_sync(0xFFFFFFFFu, run[k], 31);
+            const i64 elast = __shfl_sync(0xFFFFFFFFu, erun, 31);
+            if (elast != EZ && (ce == EZ || less_norm<L>(ce, cm, elast, last))) {
+#pragma unroll
+                for (int k = 0; k < L; k++) cm[k] = last[k];
+                ce = elast;
+            }
         }
+        const bool cond = en != EZ && (emx == EZ || less_norm<L>(emx, mx, en - eps_shift, c));
+        const unsigned hit = __ballot_sync(0xFFFFFFFFu, cond);
+        if (hit) sz = top - (31 - __clz(hit));               // the highest lane with the condition = lowest d
     }
-    if (!any) sz = 0;
-    size[t] = sz;
-    i64 tl = 3;
-    if (sz > 0) {
-        tl = 2 * (i64)(sz - 1);
-        for (int d = 0; d < sz; d++) {
+    const int kept = sz < 0 ? 0 : sz + 1;
+    // text length: the kept numbers quoted (length + 2) and joined by ",\n"; "\"0\"" for an all-zero polynomial
+    i64 tl = 0;
+    bool bad = false;
+    for (int d0 = 0; d0 < kept; d0 += 32) {
+        const int d = d0 + lane;
+        if (d < kept) {
             const int l = len[base + d];
-            if (l < 0) { tl = -1; break; }                  // a kept number the formatter could not print
-            tl += l + 2;
+            if (l < 0) bad = true;
+            else tl += l + 2;
         }
     }
-    text_len[t] = tl;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) tl += __shfl_down_sync(0xFFFFFFFFu, tl, off);
+    bad = __any_sync(0xFFFFFFFFu, bad);
+    if (lane == 0) {
+        size[t] = kept;
+        text_len[t] = kept == 0 ? 3 : (bad ? -1 : tl + 2 * (i64)(kept - 1));
+    }
 }
 
 #endif
@@ -361,7 +413,7 @@ template <int L>
 int DecimalLaunch<L>::poly_sizes(const int32_t* m, const i64* e, i64 plane, const i64* poly_num, i64 npoly, int D,
                                  int eps_shift, const int32_t* len, int32_t* size, i64* text_len, cudaStream_t st) {
     if (npoly == 0) return 0;
-    const i64 blocks = (npoly + 127) / 128;
+    const i64 blocks = (npoly + 3) / 4;                      // one warp per polynomial
     k_poly_sizes<L><<<(unsigned)blocks, 128, 0, st>>>(m, e, plane, poly_num, npoly, D, eps_shift, len, size, text_len);
     return (int)cudaGetLastError();
 }

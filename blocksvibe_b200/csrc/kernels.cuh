@@ -469,6 +469,128 @@ __global__ void __launch_bounds__(kCauchyThreads, 3) k_cauchy3(const int32_t* __
     oe[t] = eo;
 }
 
+// The Cauchy step of k_cauchy3 on sign-magnitude columns (k_cauchy_align_sm: |x| with the sign in the top bit
+// of limb L - 1), read limb by limb from memory as the division reaches them instead of held in registers: the
+// same quotient digits from the top of the same dividend |x| 2^32, so the results are bit-identical to
+// k_cauchy3, with a third of its registers per thread (more resident warps to hide the multiply-high chains).
+template <int L>
+__device__ __forceinline__ u32 sm_dividend_limb(const int32_t* __restrict__ xm, i64 plane, i64 idx, int k) {
+    if (k <= 0 || k > L) return 0u;                          // dividend limb k = |x| limb k - 1; limb 0 is zero
+    const u32 v = (u32)__ldg(xm + (i64)(k - 1) * plane + idx);
+    return k == L ? (v & 0x7FFFFFFFu) : v;
+}
+
+template <int L>
+__device__ __forceinline__ u32 sm_dividend_bits(const int32_t* __restrict__ xm, i64 plane, i64 idx, int lo, int width) {
+    const int li = lo >> 5, bo = lo & 31;
+    const u32 v0 = sm_dividend_limb<L>(xm, plane, idx, li);
+    const u32 v = bo ? ((v0 >> bo) | (sm_dividend_limb<L>(xm, plane, idx, li + 1) << (32 - bo))) : v0;
+    return width >= 32 ? v : (v & ((1u << width) - 1u));
+}
+
+template <int L, int W>
+__global__ void __launch_bounds__(kCauchyThreads, 4) k_cauchy4(const int32_t* __restrict__ xm, const i64* __restrict__ xe, i64 xplane,
+                          const int32_t* __restrict__ hm, const i64* __restrict__ he, i64 hplane,
+                          CauchyLevel lv, int32_t* __restrict__ om, i64* __restrict__ oe, i64 oplane) {
+    constexpr int TB = 32 * (L + 1), ND = (TB + W - 1) / W;
+    i64 t = blockIdx.x * (i64)blockDim.x + threadIdx.x;
+    const i64 N = lv.N;
+    if (t >= lv.nb * lv.Mr * N) return;
+    const i64 n = t % N, r = (t / N) % lv.Mr, g = t / (N * lv.Mr);
+    if (r >= lv.nrow[g]) {
+        u32 z[L];
+        zero(z);
+        store_signed<L>(om, oplane, t, z, false);
+        oe[t] = EZ;
+        return;
+    }
+    const i64 hidx = ((lv.gsrc[g] * lv.hlevels + lv.m) * lv.Jh + lv.gj[g]) * N + n;
+    const i64 E = xe[g * N + n];
+    const i64 ncol = lv.ncol[g];
+    const i64* cold = lv.cold + g * lv.Kc;
+    const i64 D = lv.rowd[g * lv.Mr + r];
+    extern __shared__ int c4_acc[];                      // (ND, blockDim.x): this thread's digit sums
+    int* acc = c4_acc + threadIdx.x;
+#pragma unroll
+    for (int j = 0; j < ND; j++) acc[j * kCauchyThreads] = 0;
+    if (E != EZ) {
+        for (i64 i = 0; i < ncol; i += 2) {
+            const bool two = i + 1 < ncol;
+            const i64 ix0 = (g * lv.Kc + i) * N + n, ix1 = two ? ix0 + N : ix0;
+            const bool n0 = ((u32)__ldg(xm + (i64)(L - 1) * xplane + ix0) >> 31) != 0;
+            const bool n1 = ((u32)__ldg(xm + (i64)(L - 1) * xplane + ix1) >> 31) != 0;
+            i64 d0 = D - cold[i], d1 = two ? D - cold[i + 1] : 0;
+            const int s0 = d0 == 0 ? 0 : ((n0 != (d0 < 0)) ? -1 : 1);
+            const int s1 = d1 == 0 ? 0 : ((n1 != (d1 < 0)) ? -1 : 1);
+            const u32 v0 = d0 == 0 ? 1u : (u32)(d0 < 0 ? -d0 : d0), v1 = d1 == 0 ? 1u : (u32)(d1 < 0 ? -d1 : d1);
+            // inv = floor(2^32 / d) (2^32 - 1 for d = 1): the estimate umulhi(c, inv) is the quotient or one below it
+            const u32 i0 = v0 == 1u ? 0xFFFFFFFFu : (u32)(0x100000000ull / v0);
+            const u32 i1 = v1 == 1u ? 0xFFFFFFFFu : (u32)(0x100000000ull / v1);
+            u32 r0 = 0, r1 = 0;
+#pragma unroll
+            for (int j = 0; j < ND; j++) {                  // digit j from the top: dividend bits [lo, lo + width)
+                const int lo = W * (ND - 1 - j);
+                const int width = j == 0 ? TB - W * (ND - 1) : W;
+                const u32 c0 = (r0 << width) | sm_dividend_bits<L>(xm, xplane, ix0, lo, width);
+                const u32 c1 = (r1 << width) | sm_dividend_bits<L>(xm, xplane, ix1, lo, width);
+                u32 q0 = umulhi32(c0, i0), q1 = umulhi32(c1, i1);
+                r0 = c0 - q0 * v0;
+                r1 = c1 - q1 * v1;
+                const bool x0 = r0 >= v0, x1 = r1 >= v1;
+                q0 += x0; r0 -= x0 ? v0 : 0u;
+                q1 += x1; r1 -= x1 ? v1 : 0u;
+                acc[j * kCauchyThreads] += s0 * (int)q0 + s1 * (int)q1;
+            }
+        }
+    }
+    // digit sums -> signed limb sums (value sum_j acc[j] 2^(W (ND - 1 - j))), carried into limbs
+    long long accl[L + 2];
+#pragma unroll
+    for (int k = 0; k < L + 2; k++) accl[k] = 0;
+    {
+        long long carry = 0;
+#pragma unroll
+        for (int j = ND - 1; j >= 0; j--) {
+            const int lo = W * (ND - 1 - j), k0 = lo >> 5, b0 = lo & 31;
+            const long long v = (long long)acc[j * kCauchyThreads] + carry;
+            long long part;
+            if (j > 0) {
+                part = v & ((1ll << W) - 1);
+                carry = v >> W;
+            } else {
+                part = v;
+            }
+            const long long lo32 = b0 ? ((part & ((1ll << (32 - b0)) - 1)) << b0) : (part & 0xFFFFFFFFll);
+            const long long hi = b0 ? (part >> (32 - b0)) : (part >> 32);
+            accl[k0] += lo32;
+            accl[k0 + 1] += hi;
+        }
+    }
+    u32 w[L + 3];
+    long long c = 0;
+#pragma unroll
+    for (int k = 0; k < L + 2; k++) {
+        long long v = accl[k] + c;
+        w[k] = (u32)v;
+        c = v >> 32;
+    }
+    w[L + 2] = (u32)c;
+    const bool neg = (w[L + 2] >> 31) != 0;
+    if (neg) negate(w);
+    u32 sres[L];
+    i64 es;
+    bool ns = false;
+    if (E != EZ && round_mag<L>(w, E - 31, sres, &es)) ns = neg;
+    else { zero(sres); es = EZ; }
+    u32 h[L], out[L];
+    const bool nh = load_mag<L>(hm, hplane, hidx, h);
+    bool no;
+    i64 eo;
+    add_norm<L>(sres, ns, es, h, nh, he[hidx], out, &no, &eo);
+    store_signed<L>(om, oplane, t, out, no);
+    oe[t] = eo;
+}
+
 // ------------------------------------------------------------------------------------------------
 // The pole kernels keep their 2 L + 2 accumulator limbs in shared memory (one column per thread), so that only
 // the operands live in registers: more resident warps to hide the latency of the multiply-add chains.
@@ -805,6 +927,8 @@ struct Launch {
                        const CauchyLevel& lv, int32_t* om, i64* oe, i64 oplane, cudaStream_t st);
     static int cauchy3(const int32_t* xm, const i64* xe, i64 xplane, const int32_t* hm, const i64* he, i64 hplane,
                        const CauchyLevel& lv, i64 dmax, int32_t* om, i64* oe, i64 oplane, cudaStream_t st);
+    static int cauchy4(const int32_t* xm, const i64* xe, i64 xplane, const int32_t* hm, const i64* he, i64 hplane,
+                       const CauchyLevel& lv, i64 dmax, int32_t* om, i64* oe, i64 oplane, cudaStream_t st);
     static int pole(const int32_t* hm, const i64* he, i64 hplane, const int32_t* Rm, const i64* Re, i64 Rplane,
                     const int32_t* Qm, const i64* Qe, i64 Qplane, const i64* t_hrow, const i64* t_R, const i64* t_qL,
                     const i64* t_slot, i64 T, i64 B, int S, int32_t* ym, i64* ye, i64 yplane,
@@ -890,6 +1014,24 @@ int Launch<L>::cauchy3(const int32_t* xm, const i64* xe, i64 xplane, const int32
             xm, xe, xplane, hm, he, hplane, lv, om, oe, oplane);
     else
         k_cauchy2<L><<<grid_for(n, kThreads), kThreads, 0, st>>>(xm, xe, xplane, hm, he, hplane, lv, om, oe, oplane);
+    return (int)cudaGetLastError();
+}
+
+template <int L>
+int Launch<L>::cauchy4(const int32_t* xm, const i64* xe, i64 xplane, const int32_t* hm, const i64* he, i64 hplane,
+                       const CauchyLevel& lv, i64 dmax, int32_t* om, i64* oe, i64 oplane, cudaStream_t st) {
+    i64 n = lv.nb * lv.Mr * lv.N;
+    if (n == 0) return 0;
+    constexpr int TB = 32 * (L + 1);
+    if (dmax < (1 << 8) && lv.Kc < 128)
+        k_cauchy4<L, 24><<<grid_for(n, kCauchyThreads), kCauchyThreads, ((TB + 23) / 24) * kCauchyThreads * 4, st>>>(
+            xm, xe, xplane, hm, he, hplane, lv, om, oe, oplane);
+    else if (dmax < (1 << 10) && lv.Kc < 512)
+        k_cauchy4<L, 22><<<grid_for(n, kCauchyThreads), kCauchyThreads, ((TB + 21) / 22) * kCauchyThreads * 4, st>>>(
+            xm, xe, xplane, hm, he, hplane, lv, om, oe, oplane);
+    else
+        k_cauchy4<L, 16><<<grid_for(n, kCauchyThreads), kCauchyThreads, ((TB + 15) / 16) * kCauchyThreads * 4, st>>>(
+            xm, xe, xplane, hm, he, hplane, lv, om, oe, oplane);
     return (int)cudaGetLastError();
 }
 

@@ -17,6 +17,10 @@ from . import _lib, mpf, structure as S
 from .mpf import MPF
 
 
+# default Cauchy kernel (see Recursion)
+CAUCHY = "cuda3"
+
+
 def _dev(a, device):
     return torch.as_tensor(np.ascontiguousarray(a), dtype=torch.int64).to(device)
 
@@ -25,13 +29,14 @@ class Recursion:
     """Numbers of one Plan on the GPU.  M: dict key -> matrix of decimal strings (keys as plan.Mkeys),
     an MPF table (nM, Smax, Smax) in plan.Mkeys order, or None for random O(1) matrices (timing runs)."""
 
-    def __init__(self, plan, M, L, device="cuda", generator=None, cauchy="cuda3", rns_min_k=32):
+    def __init__(self, plan, M, L, device="cuda", generator=None, cauchy=None, rns_min_k=32):
         """cauchy: "cuda" (one-limb divisions on the CUDA cores, b3d_cauchy_level), "cuda2" (the same quotients from
         pre-aligned columns, two per thread, b3d_cauchy_align + b3d_cauchy_level2: bit-identical to "cuda"), "cuda3"
-        (cuda2 with 24- or 22-bit quotient digits when the plan's divisors allow, b3d_cauchy_level3: bit-identical), "rns"
+        (cuda2 with 24- or 22-bit quotient digits when the plan's divisors allow, b3d_cauchy_level3: bit-identical), "cuda4"
+        (cuda3 on sign-magnitude columns read limb by limb, b3d_cauchy_align_sm + b3d_cauchy_level4: bit-identical), "rns"
         (the level's Cauchy GEMM on the tensor cores, residues + CRT), or "auto" (rns for levels with at least
         rns_min_k columns, cuda2 below)"""
-        self.cauchy, self.rns_min_k = cauchy, rns_min_k
+        self.cauchy, self.rns_min_k = cauchy or CAUCHY, rns_min_k
         self._side = {}                                  # calling stream -> stream of the per-level hook
         self.overlap_hook = True
         if not _lib.lib().b3d_supported_limbs(L):
@@ -101,7 +106,7 @@ class Recursion:
         return self._ctable
 
     def _use_rns(self, lev):
-        if self.cauchy in ("cuda", "cuda2", "cuda3") or lev["m"] == 0 or lev["Kc"] > 256:
+        if self.cauchy in ("cuda", "cuda2", "cuda3", "cuda4") or lev["m"] == 0 or lev["Kc"] > 256:
             return False
         return self.cauchy == "rns" or lev["Kc"] >= self.rns_min_k
 
@@ -188,6 +193,14 @@ class Recursion:
                                     p(lev["cold"]), p(lev["ncol"]), p(lev["col"]))
             if self._use_rns(lev):
                 self._cauchy_rns(lev, tabs, res, h_inf, H, stream)
+            elif self.cauchy == "cuda4" and lev["m"] > 0:
+                nb, Kc = lev["nb"], lev["Kc"]
+                Xm = torch.empty((L, nb * Kc * N), dtype=torch.int32, device=dev)
+                Xe = torch.empty((nb, N), dtype=torch.int64, device=dev)
+                _lib.call("b3d_cauchy_align_sm", L, p(res.m), p(res.e), res.m.stride(0), _lib.ctypes_byref(tabs), p(Xm),
+                          p(Xe), Xm.stride(0), stream)
+                _lib.call("b3d_cauchy_level4", L, p(Xm), p(Xe), Xm.stride(0), p(h_inf.m), p(h_inf.e),
+                          h_inf.m.stride(0), _lib.ctypes_byref(tabs), plan.dmax, p(H.m), p(H.e), H.m.stride(0), stream)
             elif self.cauchy in ("cuda2", "cuda3") and lev["m"] > 0:
                 nb, Kc = lev["nb"], lev["Kc"]
                 Xm = torch.empty((L, nb * Kc * N), dtype=torch.int32, device=dev)

@@ -219,6 +219,18 @@ int b3d_cauchy_level3(int L, const int32_t* xm, const int64_t* xe, int64_t xplan
                       const int64_t* he, int64_t hplane, const b3d_level_tables* lv, int64_t dmax, int32_t* om,
                       int64_t* oe, int64_t oplane, void* stream);
 
+/* b3d_cauchy_align with sign-magnitude output (|x| aligned, its sign in bit 31 of limb L - 1): the input of
+ * b3d_cauchy_level4 */
+int b3d_cauchy_align_sm(int L, const int32_t* rm, const int64_t* re, int64_t rplane, const b3d_level_tables* lv,
+                        int32_t* om, int64_t* oe, int64_t oplane, void* stream);
+
+/* b3d_cauchy_level3 on the sign-magnitude columns of b3d_cauchy_align_sm, each column's limbs read from memory
+ * as the division reaches them (fewer registers per thread); results bit-identical to b3d_cauchy_level3
+ * (replaces cauchy.cauchy, cauchy.py:73-87, like it) */
+int b3d_cauchy_level4(int L, const int32_t* xm, const int64_t* xe, int64_t xplane, const int32_t* hm,
+                      const int64_t* he, int64_t hplane, const b3d_level_tables* lv, int64_t dmax, int32_t* om,
+                      int64_t* oe, int64_t oplane, void* stream);
+
 /* digit matrices of C (as b3d_rns_split writes them) from table[(d + dmax) * np + j] = residues of
  * round(2^(NB-1) / d) */
 int b3d_cauchy_digits(const b3d_level_tables* lv, const uint32_t* table, int64_t dmax, int np, int64_t Rp, int64_t Kp,

@@ -118,12 +118,13 @@ def test_slot_reuse_same_live_residues(cuda):
     (2, 2, 60, 50, ((0, 0), (1, 1)), 10, 1, 63),            # divisors up to 314: 22-bit digits in cuda3
 ])
 def test_cauchy_forms_bitwise_equal(cuda, case):
-    """the pre-aligned two-terms-per-thread Cauchy kernel and its wide-digit form give the first kernel's bits"""
+    """the pre-aligned two-terms-per-thread Cauchy kernel, its wide-digit form and the wide-digit form on
+    sign-magnitude columns read limb by limb give the first kernel's bits"""
     tj12, tj43, tjmax, order, pp, L, nrhs, seed = case
     M, H = random_case(*case)
     plan = PL.Plan(tj12, tj43, tjmax, order, pp, reuse=True)
     outs = []
-    for form in ("cuda", "cuda2", "cuda3"):
+    for form in ("cuda", "cuda2", "cuda3", "cuda4"):
         rec = RC.Recursion(plan, M, L, device=cuda, cauchy=form)
         outs.append(rec.run(hinf_tensor(H, plan, order, nrhs, L, cuda)))
     for o in outs[1:]:
