@@ -810,100 +810,146 @@ __global__ void __launch_bounds__(kMomThreads, 3) k_moments_stage(const int32_t*
     ye[out] = ey;
 }
 
-// One lane per moment order kk: a warp serves floor(32 / R1) (row, column) items, every lane of an item reading
-// the same staged numbers (broadcast loads) and forming its own order's exact window sum.  nk: n^kk as KW
-// little-endian 32-bit limbs, nk[(kk * NN + n) * KW + j]; nkb[kk * NN + n] its bit length (0 for 0^kk, kk > 0).
-template <int L, int KW>
-__global__ void __launch_bounds__(kMomThreads) k_moments_flush(const int32_t* __restrict__ ym, const i64* __restrict__ ye,
+// One thread per (row, column) item, the moment orders in chunks of kFlushKC: for each staged term, the exact
+// product |Y| n^k0 (n^k0 from the table nk: nk[(k * NN + n) * KW + j], 32-bit limbs; nkb[k * NN + n] its bit
+// length), then times n for each further order of the chunk, each added into that order's accumulator (a
+// shared-memory column of L + 3 words, two's complement) at the word and bit offset of its exponent: no barrel
+// shifter, one funnel shift per word.  The accumulator of order k keeps the bits from 32 (L + 2) below the bound
+// E_k = max_w (e_w + NB + bits(n_w^k)) of its terms (truncated below), then rounds once.
+constexpr int kFlushThreads = 64;
+constexpr int kFlushKC = 4;
+
+template <int L, int NP>
+__device__ __forceinline__ void add_at_offset(u32* acc, int stride, const u32 (&P)[NP], i64 off, bool neg) {
+    constexpr int ACC = L + 3;
+    const i64 qq = off >= 0 ? off / 32 : -((-off + 31) / 32);      // floor(off / 32)
+    const int f = (int)(off - 32 * qq);
+    const int q = (int)qq;
+    u32 carry = 0;                                                  // carry (add) or borrow (subtract)
+#pragma unroll
+    for (int j = 0; j <= NP; j++) {
+        const int a = j + q;
+        const u32 lo = j > 0 ? P[j - 1] : 0u, hi = j < NP ? P[j] : 0u;
+        const u32 v = fsl(lo, hi, f);                               // word j of P 2^f
+        if (a < 0 || a >= ACC) continue;                            // below the accumulator: truncated
+        const u32 w = acc[a * stride];
+        if (!neg) {
+            const u32 s1 = w + v, s2 = s1 + carry;
+            carry = (s1 < w) | (s2 < s1);
+            acc[a * stride] = s2;
+        } else {
+            const u32 d1 = w - v, d2 = d1 - carry;
+            carry = (w < v) | (d1 < carry);
+            acc[a * stride] = d2;
+        }
+    }
+    for (int a = NP + 1 + q; carry && a < ACC; a++) {              // propagate to the top
+        if (a < 0) continue;
+        const u32 w = acc[a * stride];
+        if (!neg) { acc[a * stride] = w + 1; carry = w == 0xFFFFFFFFu; }
+        else { acc[a * stride] = w - 1; carry = w == 0u; }
+    }
+}
+
+template <int L, int KW, bool ACCUMULATE>
+__global__ void __launch_bounds__(kFlushThreads) k_moments_flush(const int32_t* __restrict__ ym, const i64* __restrict__ ye,
                           i64 yplane, const i64* __restrict__ row_shift, i64 m0, int W, i64 rows, i64 N, int R1,
-                          const u32* __restrict__ nk, const int32_t* __restrict__ nkb, int NN, int accumulate,
+                          const u32* __restrict__ nk, const int32_t* __restrict__ nkb, int NN,
                           int32_t* __restrict__ mm, i64* __restrict__ me, i64 mplane) {
     constexpr int NB = nb_bits(L);
-    constexpr int ACC = L + 3;                           // two's complement; magnitudes below 2^(32 (L + 2))
-    const int lane = threadIdx.x & 31, per = 32 / R1;
-    const int sub = lane / R1, kk = lane - sub * R1;
-    if (sub >= per) return;
-    const i64 item = ((blockIdx.x * (i64)blockDim.x + threadIdx.x) >> 5) * per + sub;
+    constexpr int ACC = L + 3;
+    constexpr int NP = L + KW + 1;                       // |Y| n^k, k within a chunk: n^k0 < 2^(32 KW), n^3 < 2^32
+    extern __shared__ u32 flush_acc[];                   // (kFlushKC * ACC, blockDim.x)
+    const i64 item = blockIdx.x * (i64)blockDim.x + threadIdx.x;
     if (item >= rows * N) return;
     const i64 row = item / N, c = item - row * N;
     const i64 sh = row_shift[row];
-    i64 E = EZ;                                          // bound on the top bit of the window's terms
-    for (int w = 0; w < W; w++) {
-        const i64 ey = ye[(w * rows + row) * N + c];
-        const i64 n = m0 + w + sh;
-        if (ey == EZ || n >= NN) continue;
-        const int kb = nkb[kk * NN + n];
-        if (kb == 0) continue;
-        const i64 top = ey + NB + kb;
-        if (top > E) E = top;
-    }
-    const i64 o = (row * R1 + kk) * N + c;
-    if (E == EZ) {
-        if (!accumulate) {
+    u32* acc = flush_acc + threadIdx.x;
+    for (int k0 = 0; k0 < R1; k0 += kFlushKC) {
+        const int kc = R1 - k0 < kFlushKC ? R1 - k0 : kFlushKC;
+        i64 E[kFlushKC];
 #pragma unroll
-            for (int k = 0; k < L; k++) mm[k * mplane + o] = 0;
-            me[o] = EZ;
-        }
-        return;
-    }
-    const i64 base = E - 32 * (L + 2);                   // weight of the accumulator's lowest bit
-    u32 acc[ACC];
-    zero(acc);
-    for (int w = 0; w < W; w++) {
-        const i64 ix = (w * rows + row) * N + c;
-        const i64 ey = ye[ix];
-        const i64 n = m0 + w + sh;
-        if (ey == EZ || n >= NN) continue;
-        if (nkb[kk * NN + n] == 0) continue;
-        u32 y[L];
-        const bool neg = load_mag<L>(ym, yplane, ix, y);
-        u32 P[L + KW];                                   // |Y| n^kk, exact
-        zero(P);
+        for (int kk = 0; kk < kFlushKC; kk++) E[kk] = EZ;
+        for (int w = 0; w < W; w++) {
+            const i64 ey = ye[(w * rows + row) * N + c];
+            const i64 n = m0 + w + sh;
+            if (ey == EZ || n >= NN) continue;
 #pragma unroll
-        for (int j = 0; j < KW; j++) {
-            const u32 b = nk[((i64)kk * NN + n) * KW + j];
-            u32 carry = 0;
-#pragma unroll
-            for (int i = 0; i < L; i++) {
-                const u64 v = (u64)y[i] * b + P[i + j] + carry;
-                P[i + j] = (u32)v;
-                carry = (u32)(v >> 32);
-            }
-#pragma unroll
-            for (int i = L + j; i < L + KW; i++) {
-                const u64 v = (u64)P[i] + carry;
-                P[i] = (u32)v;
-                carry = (u32)(v >> 32);
+            for (int kk = 0; kk < kFlushKC; kk++) {
+                if (kk >= kc) break;
+                const int kb = nkb[(k0 + kk) * NN + n];
+                if (kb && ey + NB + kb > E[kk]) E[kk] = ey + NB + kb;
             }
         }
-        const i64 off = ey - base;                       // bit position of P's lowest bit in the accumulator
-        u32 T[ACC];
-        if (off >= 0) {
-            shl(P, (int)off, T);
-        } else if (-off < 32 * (L + KW)) {
-            shr(P, (int)(-off), T);
-        } else {
-            continue;
+        for (int k = 0; k < kFlushKC * ACC; k++) acc[k * kFlushThreads] = 0;
+        for (int w = 0; w < W; w++) {
+            const i64 ix = (w * rows + row) * N + c;
+            const i64 ey = ye[ix];
+            const i64 n = m0 + w + sh;
+            if (ey == EZ || n >= NN) continue;
+            u32 y[L];
+            const bool neg = load_mag<L>(ym, yplane, ix, y);
+            u32 P[NP];
+            zero(P);
+#pragma unroll
+            for (int j = 0; j < KW; j++) {               // P = |Y| n^k0
+                const u32 b = nk[((i64)k0 * NN + n) * KW + j];
+                u32 carry = 0;
+#pragma unroll
+                for (int i = 0; i < L; i++) {
+                    const u64 v = (u64)y[i] * b + P[i + j] + carry;
+                    P[i + j] = (u32)v;
+                    carry = (u32)(v >> 32);
+                }
+                P[L + j] += carry;
+            }
+#pragma unroll 1
+            for (int kk = 0; kk < kc; kk++) {
+                if (kk > 0) {                            // P *= n (exact)
+                    u32 carry = 0;
+#pragma unroll
+                    for (int i = 0; i < NP; i++) {
+                        const u64 v = (u64)P[i] * (u64)n + carry;
+                        P[i] = (u32)v;
+                        carry = (u32)(v >> 32);
+                    }
+                }
+                if (E[kk] == EZ || nkb[(k0 + kk) * NN + n] == 0) continue;
+                add_at_offset<L, NP>(acc + kk * ACC * kFlushThreads, kFlushThreads, P, ey - (E[kk] - 32 * (L + 2)), neg);
+            }
         }
-        add_signed(acc, T, neg);
-    }
-    const bool neg = (acc[ACC - 1] >> 31) != 0;
-    if (neg) negate(acc);
-    u32 r[L];
-    i64 er;
-    bool nr = neg;
-    if (!round_mag<L>(acc, base, r, &er)) nr = false;
-    if (accumulate) {
-        u32 v[L], sum[L];
-        const bool nv = load_mag<L>(mm, mplane, o, v);
-        bool ns;
-        i64 es;
-        add_norm<L>(v, nv, me[o], r, nr, er, sum, &ns, &es);
-        store_signed<L>(mm, mplane, o, sum, ns);
-        me[o] = es;
-    } else {
-        store_signed<L>(mm, mplane, o, r, nr);
-        me[o] = er;
+        for (int kk = 0; kk < kc; kk++) {
+            const i64 o = (row * R1 + k0 + kk) * N + c;
+            if (E[kk] == EZ) {
+                if (!ACCUMULATE) {
+#pragma unroll
+                    for (int k = 0; k < L; k++) mm[k * mplane + o] = 0;
+                    me[o] = EZ;
+                }
+                continue;
+            }
+            u32 mag[ACC];
+#pragma unroll
+            for (int k = 0; k < ACC; k++) mag[k] = acc[(kk * ACC + k) * kFlushThreads];
+            const bool negs = (mag[ACC - 1] >> 31) != 0;
+            if (negs) negate(mag);
+            u32 r[L];
+            i64 er;
+            bool nr = negs;
+            if (!round_mag<L>(mag, E[kk] - 32 * (L + 2), r, &er)) nr = false;
+            if (ACCUMULATE) {
+                u32 v[L], sum[L];
+                const bool nv = load_mag<L>(mm, mplane, o, v);
+                bool ns;
+                i64 es;
+                add_norm<L>(v, nv, me[o], r, nr, er, sum, &ns, &es);
+                store_signed<L>(mm, mplane, o, sum, ns);
+                me[o] = es;
+            } else {
+                store_signed<L>(mm, mplane, o, r, nr);
+                me[o] = er;
+            }
+        }
     }
 }
 
@@ -1078,14 +1124,13 @@ int Launch<L>::moments_flush(const int32_t* ym, const i64* ye, i64 yplane, const
                              int32_t* mm, i64* me, i64 mplane, cudaStream_t st) {
     const i64 items = rows * N;
     if (items == 0 || W == 0) return 0;
-    const int per = 32 / R1;
-    const i64 warps = (items + per - 1) / per;
-    const unsigned grid = (unsigned)((warps * 32 + kMomThreads - 1) / kMomThreads);
-#define B3D_FLUSH(KWC) k_moments_flush<L, KWC><<<grid, kMomThreads, 0, st>>>(ym, ye, yplane, row_shift, m0, W, rows, N, R1, \
-                                                                         nk, nkb, NN, accumulate, mm, me, mplane)
-    if (KW <= 2) B3D_FLUSH(2);
-    else if (KW <= 6) B3D_FLUSH(6);
-    else B3D_FLUSH(12);
+    const unsigned grid = (unsigned)((items + kFlushThreads - 1) / kFlushThreads);
+    const int smem = kFlushThreads * kFlushKC * (L + 3) * 4;
+#define B3D_FLUSH(KWC, AC) k_moments_flush<L, KWC, AC><<<grid, kFlushThreads, smem, st>>>(ym, ye, yplane, row_shift, m0, W, \
+                                                                             rows, N, R1, nk, nkb, NN, mm, me, mplane)
+    if (KW <= 2) { if (accumulate) B3D_FLUSH(2, true); else B3D_FLUSH(2, false); }
+    else if (KW <= 6) { if (accumulate) B3D_FLUSH(6, true); else B3D_FLUSH(6, false); }
+    else { if (accumulate) B3D_FLUSH(12, true); else B3D_FLUSH(12, false); }
 #undef B3D_FLUSH
     return (int)cudaGetLastError();
 }

@@ -18,7 +18,7 @@ from .mpf import MPF
 
 
 # default Cauchy kernel (see Recursion)
-CAUCHY = "cuda3"
+CAUCHY = "cuda4"
 
 
 def _dev(a, device):
