@@ -12,7 +12,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libb3dgpu.so")
 BUILD = os.path.join(ROOT, "_build")
-LIMBS = (6, 10, 18, 26, 30, 34, 42)
+LIMBS = (6, 10, 14, 18, 22, 26, 30, 34, 38, 42, 46)
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-I", os.path.join(ROOT, "include"), "-I", CSRC]
 

@@ -41,7 +41,7 @@ const char* b3d_last_error(void) { return b3d::g_error.c_str(); }
 
 int b3d_supported_limbs(int L) {
     switch (L) {
-        case 6: case 10: case 18: case 26: case 30: case 34: case 42: return 1;
+        case 6: case 10: case 14: case 18: case 22: case 26: case 30: case 34: case 38: case 42: case 46: return 1;
         default: return 0;
     }
 }
@@ -120,11 +120,20 @@ int b3d_moments_stage(int L, const int32_t* rm, const int64_t* re, int64_t rplan
 
 int b3d_moments_flush(int L, const int32_t* ym, const int64_t* ye, int64_t yplane, const int64_t* row_shift, int64_t m0,
                       int W, int64_t rows, int64_t N, int R1, const uint32_t* nk, const int32_t* nkb, int NN, int KW,
-                      int accumulate, int32_t* mm, int64_t* me, int64_t mplane, void* stream) {
+                      int accumulate, int Lout, int32_t* mm, int64_t* me, int64_t mplane, void* stream) {
     if (!nonneg(rows) || !nonneg(N) || !nonneg(m0) || W < 0 || R1 < 1 || R1 > 32 || NN < 1 || KW < 1 || KW > 12)
         return fail(B3D_E_ARG, "b3d_moments_flush: invalid size (1 <= R + 1 <= 32, 1 <= KW <= 12)");
+    if ((Lout != L && Lout != L + 4) || !b3d_supported_limbs(Lout))
+        return fail(B3D_E_ARG, "b3d_moments_flush: Lout must be L or L + 4 (compiled)");
     B3D_DISPATCH(L, cuda_status(LX::moments_flush(ym, ye, yplane, row_shift, m0, W, rows, N, R1, nk, nkb, NN, KW,
-                                                 accumulate, mm, me, mplane, as_stream(stream)), "b3d_moments_flush"));
+                                                 accumulate, Lout, mm, me, mplane, as_stream(stream)), "b3d_moments_flush"));
+}
+
+int b3d_resize(int L, const int32_t* m, const int64_t* e, int64_t plane, int64_t n, int Lout, int32_t* om, int64_t* oe,
+               int64_t oplane, void* stream) {
+    if (!nonneg(n) || (Lout != L && Lout != L + 4 && Lout != L - 4) || !b3d_supported_limbs(Lout))
+        return fail(B3D_E_ARG, "b3d_resize: Lout must be L or L +- 4 (compiled)");
+    B3D_DISPATCH(L, cuda_status(LX::resize(m, e, plane, n, Lout, om, oe, oplane, as_stream(stream)), "b3d_resize"));
 }
 
 namespace {
@@ -155,7 +164,7 @@ int b3d_rns_split_mma(int L, const b3d_rns_split_args* a, const b3d_rns_tables* 
     if (!a || !tb || tb->np != b3d::rns_primes(L) || a->nb < 0 || a->nb > 65535 || a->R < 0 || a->K < 0 ||
         a->Rp < a->R || a->Kp < a->K || a->Kp % 32 || a->TR % 16 || a->TR <= 0 || (4 * a->Rp) % a->TR ||
         a->mat_bytes < 4 * a->Rp * a->Kp || a->Ks % 32 || a->Ks < 4 * L || a->NS % 16 || a->NS <= 0 ||
-        a->NS > 256 || 2 * a->NS < 4 * tb->np || 128 * a->Ks + 2 * a->NS * a->Ks + tb->np * 512 > 200 * 1024)
+        a->NS > 256 || 2 * a->NS < 4 * tb->np || 128 * a->Ks + 2 * a->NS * a->Ks + tb->np * 512 > b3d::kRnsSmemCap)
         return fail(B3D_E_ARG, "b3d_rns_split_mma: invalid sizes or tables");
     b3d::RnsSplit c{a->m, a->plane, a->nb, a->R, a->K, a->sb, a->sr, a->sk, a->Rp, a->Kp, a->TR, a->mat_bytes,
                     a->out, a->C, a->Ks, a->NS, a->err};
@@ -180,7 +189,7 @@ int b3d_rns_mma(const b3d_rns_mma_args* a, const b3d_rns_tables* tb, void* strea
 int b3d_rns_crt_mma(int L, const b3d_rns_crt_args* a, const b3d_rns_tables* tb, void* stream) {
     if (!a || !tb || tb->np != b3d::rns_primes(L) || tb->ml != b3d::rns_mlimbs(L) || a->Kc % 32 ||
         a->Kc < 4 * tb->np || a->NH % 16 || a->NH <= 0 || a->NH > 256 || 2 * a->NH < 4 * tb->ml + 3 ||
-        (128 + 2 * a->NH) * a->Kc > 200 * 1024 || a->n != a->nbatch * a->M * a->N || a->n < 0)
+        (128 + 2 * a->NH) * a->Kc > b3d::kRnsSmemCap || a->n != a->nbatch * a->M * a->N || a->n < 0)
         return fail(B3D_E_ARG, "b3d_rns_crt_mma: invalid sizes or tables");
     b3d::RnsCrt c{a->A, a->T, a->Kc, a->NH, a->n, a->nbatch, a->M, a->N, a->ea, a->eb, a->cm, a->ce, a->cplane, a->err};
     b3d::RnsTables t = tables_of(tb);

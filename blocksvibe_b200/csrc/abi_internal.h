@@ -29,6 +29,10 @@ int cauchy_digits_launch(const CauchyLevel& lv, const uint32_t* table, int64_t d
         case 26: { using RX = b3d::RnsLaunch<26>; return CALL; }               \
         case 30: { using RX = b3d::RnsLaunch<30>; return CALL; }               \
         case 34: { using RX = b3d::RnsLaunch<34>; return CALL; }               \
+        case 14: { using RX = b3d::RnsLaunch<14>; return CALL; }\
+        case 22: { using RX = b3d::RnsLaunch<22>; return CALL; }\
+        case 38: { using RX = b3d::RnsLaunch<38>; return CALL; }\
+        case 46: { using RX = b3d::RnsLaunch<46>; return CALL; }\
         case 42: { using RX = b3d::RnsLaunch<42>; return CALL; }               \
         default: return b3d::fail(B3D_E_LIMBS, "no kernels compiled for L = " + std::to_string(L)); \
     }
@@ -41,6 +45,10 @@ int cauchy_digits_launch(const CauchyLevel& lv, const uint32_t* table, int64_t d
         case 26: { using CX = b3d::CauchyRnsLaunch<26>; return CALL; }         \
         case 30: { using CX = b3d::CauchyRnsLaunch<30>; return CALL; }         \
         case 34: { using CX = b3d::CauchyRnsLaunch<34>; return CALL; }         \
+        case 14: { using CX = b3d::CauchyRnsLaunch<14>; return CALL; }\
+        case 22: { using CX = b3d::CauchyRnsLaunch<22>; return CALL; }\
+        case 38: { using CX = b3d::CauchyRnsLaunch<38>; return CALL; }\
+        case 46: { using CX = b3d::CauchyRnsLaunch<46>; return CALL; }\
         case 42: { using CX = b3d::CauchyRnsLaunch<42>; return CALL; }         \
         default: return b3d::fail(B3D_E_LIMBS, "no kernels compiled for L = " + std::to_string(L)); \
     }
@@ -53,6 +61,10 @@ int cauchy_digits_launch(const CauchyLevel& lv, const uint32_t* table, int64_t d
         case 26: { using LX = b3d::Launch<26>; return CALL; }                  \
         case 30: { using LX = b3d::Launch<30>; return CALL; }                  \
         case 34: { using LX = b3d::Launch<34>; return CALL; }                  \
+        case 14: { using LX = b3d::Launch<14>; return CALL; }\
+        case 22: { using LX = b3d::Launch<22>; return CALL; }\
+        case 38: { using LX = b3d::Launch<38>; return CALL; }\
+        case 46: { using LX = b3d::Launch<46>; return CALL; }\
         case 42: { using LX = b3d::Launch<42>; return CALL; }                  \
         default: return b3d::fail(B3D_E_LIMBS, "no kernels compiled for L = " + std::to_string(L)); \
     }

@@ -56,6 +56,10 @@ __global__ void k_emit_text(const char* __restrict__ slots, int stride, const in
         case 26: { using DX = b3d::DecimalLaunch<26>; return CALL; }           \
         case 30: { using DX = b3d::DecimalLaunch<30>; return CALL; }           \
         case 34: { using DX = b3d::DecimalLaunch<34>; return CALL; }           \
+        case 14: { using DX = b3d::DecimalLaunch<14>; return CALL; }\
+        case 22: { using DX = b3d::DecimalLaunch<22>; return CALL; }\
+        case 38: { using DX = b3d::DecimalLaunch<38>; return CALL; }\
+        case 46: { using DX = b3d::DecimalLaunch<46>; return CALL; }\
         case 42: { using DX = b3d::DecimalLaunch<42>; return CALL; }           \
         default: return b3d::fail(B3D_E_LIMBS, "no kernels compiled for L = " + std::to_string(L)); \
     }

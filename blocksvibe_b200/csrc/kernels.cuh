@@ -819,9 +819,8 @@ __global__ void __launch_bounds__(kMomThreads, 3) k_moments_stage(const int32_t*
 constexpr int kFlushThreads = 64;
 constexpr int kFlushKC = 4;
 
-template <int L, int NP>
+template <int ACC, int NP>
 __device__ __forceinline__ void add_at_offset(u32* acc, int stride, const u32 (&P)[NP], i64 off, bool neg) {
-    constexpr int ACC = L + 3;
     const i64 qq = off >= 0 ? off / 32 : -((-off + 31) / 32);      // floor(off / 32)
     const int f = (int)(off - 32 * qq);
     const int q = (int)qq;
@@ -851,13 +850,13 @@ __device__ __forceinline__ void add_at_offset(u32* acc, int stride, const u32 (&
     }
 }
 
-template <int L, int KW, bool ACCUMULATE>
+template <int L, int LO, int KW, bool ACCUMULATE>
 __global__ void __launch_bounds__(kFlushThreads) k_moments_flush(const int32_t* __restrict__ ym, const i64* __restrict__ ye,
                           i64 yplane, const i64* __restrict__ row_shift, i64 m0, int W, i64 rows, i64 N, int R1,
                           const u32* __restrict__ nk, const int32_t* __restrict__ nkb, int NN,
                           int32_t* __restrict__ mm, i64* __restrict__ me, i64 mplane) {
-    constexpr int NB = nb_bits(L);
-    constexpr int ACC = L + 3;
+    constexpr int NB = nb_bits(L);                       // staged terms: L limbs; moments: LO limbs
+    constexpr int ACC = LO + 3;
     constexpr int NP = L + KW + 1;                       // |Y| n^k, k within a chunk: n^k0 < 2^(32 KW), n^3 < 2^32
     extern __shared__ u32 flush_acc[];                   // (kFlushKC * ACC, blockDim.x)
     const i64 item = blockIdx.x * (i64)blockDim.x + threadIdx.x;
@@ -915,7 +914,7 @@ __global__ void __launch_bounds__(kFlushThreads) k_moments_flush(const int32_t* 
                     }
                 }
                 if (E[kk] == EZ || nkb[(k0 + kk) * NN + n] == 0) continue;
-                add_at_offset<L, NP>(acc + kk * ACC * kFlushThreads, kFlushThreads, P, ey - (E[kk] - 32 * (L + 2)), neg);
+                add_at_offset<ACC, NP>(acc + kk * ACC * kFlushThreads, kFlushThreads, P, ey - (E[kk] - 32 * (LO + 2)), neg);
             }
         }
         for (int kk = 0; kk < kc; kk++) {
@@ -923,7 +922,7 @@ __global__ void __launch_bounds__(kFlushThreads) k_moments_flush(const int32_t* 
             if (E[kk] == EZ) {
                 if (!ACCUMULATE) {
 #pragma unroll
-                    for (int k = 0; k < L; k++) mm[k * mplane + o] = 0;
+                    for (int k = 0; k < LO; k++) mm[k * mplane + o] = 0;
                     me[o] = EZ;
                 }
                 continue;
@@ -933,24 +932,52 @@ __global__ void __launch_bounds__(kFlushThreads) k_moments_flush(const int32_t* 
             for (int k = 0; k < ACC; k++) mag[k] = acc[(kk * ACC + k) * kFlushThreads];
             const bool negs = (mag[ACC - 1] >> 31) != 0;
             if (negs) negate(mag);
-            u32 r[L];
+            u32 r[LO];
             i64 er;
             bool nr = negs;
-            if (!round_mag<L>(mag, E[kk] - 32 * (L + 2), r, &er)) nr = false;
+            if (!round_mag<LO>(mag, E[kk] - 32 * (LO + 2), r, &er)) nr = false;
             if (ACCUMULATE) {
-                u32 v[L], sum[L];
-                const bool nv = load_mag<L>(mm, mplane, o, v);
+                u32 v[LO], sum[LO];
+                const bool nv = load_mag<LO>(mm, mplane, o, v);
                 bool ns;
                 i64 es;
-                add_norm<L>(v, nv, me[o], r, nr, er, sum, &ns, &es);
-                store_signed<L>(mm, mplane, o, sum, ns);
+                add_norm<LO>(v, nv, me[o], r, nr, er, sum, &ns, &es);
+                store_signed<LO>(mm, mplane, o, sum, ns);
                 me[o] = es;
             } else {
-                store_signed<L>(mm, mplane, o, r, nr);
+                store_signed<LO>(mm, mplane, o, r, nr);
                 me[o] = er;
             }
         }
     }
+}
+
+// ------------------------------------------------------------------------------------------------
+// Change of limb count: widening is exact (the mantissa moves up by 32 (LO - LI) bits), narrowing rounds once
+// (half away from zero) to 32 LO - 2 bits.
+template <int LI, int LO>
+__global__ void k_resize(const int32_t* __restrict__ m, const i64* __restrict__ e, i64 plane, i64 n,
+                         int32_t* __restrict__ om, i64* __restrict__ oe, i64 oplane) {
+    const i64 i = blockIdx.x * (i64)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    u32 a[LI];
+    const bool neg = load_mag<LI>(m, plane, i, a);
+    const i64 ea = e[i];
+    u32 r[LO];
+    i64 er = EZ;
+    bool nr = neg;
+    if (is_zero(a) || ea == EZ) {
+        zero(r);
+        nr = false;
+    } else if (LO >= LI) {
+#pragma unroll
+        for (int k = 0; k < LO; k++) r[k] = k >= LO - LI ? a[k - (LO - LI)] : 0u;
+        er = ea - 32 * (LO - LI);
+    } else if (!round_mag<LO>(a, ea, r, &er)) {
+        nr = false;
+    }
+    store_signed<LO>(om, oplane, i, r, nr);
+    oe[i] = er;
 }
 
 // ------------------------------------------------------------------------------------------------
@@ -986,8 +1013,10 @@ struct Launch {
                              const i64* q_slot, const i64* q_row, const i64* q_n, i64 Q, i64 N, i64 w, i64 rows,
                              int32_t* ym, i64* ye, i64 yplane, cudaStream_t st);
     static int moments_flush(const int32_t* ym, const i64* ye, i64 yplane, const i64* row_shift, i64 m0, int W, i64 rows,
-                             i64 N, int R1, const u32* nk, const int32_t* nkb, int NN, int KW, int accumulate,
+                             i64 N, int R1, const u32* nk, const int32_t* nkb, int NN, int KW, int accumulate, int LO,
                              int32_t* mm, i64* me, i64 mplane, cudaStream_t st);
+    static int resize(const int32_t* m, const i64* e, i64 plane, i64 n, int LO, int32_t* om, i64* oe, i64 oplane,
+                      cudaStream_t st);
 };
 
 #ifdef B3D_DEFINE_LAUNCH
@@ -1120,23 +1149,49 @@ int Launch<L>::moments_stage(const int32_t* rm, const i64* re, i64 rplane, const
 
 template <int L>
 int Launch<L>::moments_flush(const int32_t* ym, const i64* ye, i64 yplane, const i64* row_shift, i64 m0, int W, i64 rows,
-                             i64 N, int R1, const u32* nk, const int32_t* nkb, int NN, int KW, int accumulate,
+                             i64 N, int R1, const u32* nk, const int32_t* nkb, int NN, int KW, int accumulate, int LO,
                              int32_t* mm, i64* me, i64 mplane, cudaStream_t st) {
     const i64 items = rows * N;
     if (items == 0 || W == 0) return 0;
     const unsigned grid = (unsigned)((items + kFlushThreads - 1) / kFlushThreads);
-    const int smem = kFlushThreads * kFlushKC * (L + 3) * 4;
-#define B3D_FLUSH(KWC, AC) k_moments_flush<L, KWC, AC><<<grid, kFlushThreads, smem, st>>>(ym, ye, yplane, row_shift, m0, W, \
-                                                                             rows, N, R1, nk, nkb, NN, mm, me, mplane)
-    if (KW <= 2) { if (accumulate) B3D_FLUSH(2, true); else B3D_FLUSH(2, false); }
-    else if (KW <= 6) { if (accumulate) B3D_FLUSH(6, true); else B3D_FLUSH(6, false); }
-    else { if (accumulate) B3D_FLUSH(12, true); else B3D_FLUSH(12, false); }
+#define B3D_FLUSH(LOC, KWC, AC) do {                                                                       \
+        const int smem = kFlushThreads * kFlushKC * ((LOC) + 3) * 4;     /* above 48 KB from 46 limbs: opt in */ \
+        static bool opted = false;                                                                           \
+        if (!opted) {                                                                                        \
+            const int rc = (int)cudaFuncSetAttribute(k_moments_flush<L, LOC, KWC, AC>,                      \
+                                                     cudaFuncAttributeMaxDynamicSharedMemorySize, smem);    \
+            if (rc) return rc;                                                                               \
+            opted = true;                                                                                    \
+        }                                                                                                    \
+        k_moments_flush<L, LOC, KWC, AC><<<grid, kFlushThreads, smem, st>>>(ym, ye, yplane, row_shift, m0, W, rows, N, R1, \
+                                                                            nk, nkb, NN, mm, me, mplane);    \
+    } while (0)
+#define B3D_FLUSH_KW(LOC) \
+    if (KW <= 2) { if (accumulate) B3D_FLUSH(LOC, 2, true); else B3D_FLUSH(LOC, 2, false); } \
+    else if (KW <= 6) { if (accumulate) B3D_FLUSH(LOC, 6, true); else B3D_FLUSH(LOC, 6, false); } \
+    else { if (accumulate) B3D_FLUSH(LOC, 12, true); else B3D_FLUSH(LOC, 12, false); }
+    if (LO == L) { B3D_FLUSH_KW(L) }
+    else if (LO == L + 4) { B3D_FLUSH_KW(L + 4) }
+    else return (int)cudaErrorInvalidValue;
+#undef B3D_FLUSH_KW
 #undef B3D_FLUSH
+    return (int)cudaGetLastError();
+}
+
+template <int L>
+int Launch<L>::resize(const int32_t* m, const i64* e, i64 plane, i64 n, int LO, int32_t* om, i64* oe, i64 oplane,
+                      cudaStream_t st) {
+    if (n == 0) return 0;
+    const unsigned grid = grid_for(n, kThreads);
+    if (LO == L) k_resize<L, L><<<grid, kThreads, 0, st>>>(m, e, plane, n, om, oe, oplane);
+    else if (LO == L + 4) k_resize<L, L + 4><<<grid, kThreads, 0, st>>>(m, e, plane, n, om, oe, oplane);
+    else if (LO == L - 4 && L > 4) k_resize<L, (L > 4 ? L - 4 : L)><<<grid, kThreads, 0, st>>>(m, e, plane, n, om, oe, oplane);
+    else return (int)cudaErrorInvalidValue;
     return (int)cudaGetLastError();
 }
 #endif
 
 // limb counts with compiled kernels: 2 ceil(prec / 64) + 2 for precisions 128 ... 1280 bits, plus 6
-#define B3D_FOR_EACH_L(X) X(6) X(10) X(18) X(26) X(30) X(34) X(42)
+#define B3D_FOR_EACH_L(X) X(6) X(10) X(14) X(18) X(22) X(26) X(30) X(34) X(38) X(42) X(46)
 
 }  // namespace b3d

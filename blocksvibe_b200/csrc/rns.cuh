@@ -28,6 +28,9 @@ namespace b3d {
 // number of primes and limbs of M for L-limb operands and inner dimension K <= 4096
 B3D_CX int rns_primes(int L) { return (2 * (32 * L - 2) + 12 + 2 + 30) / 31 + 1; }
 B3D_CX int rns_mlimbs(int L) { return (31 * rns_primes(L) + 31) / 32 + 1; }
+// dynamic shared memory cap of the tensor-core split and CRT kernels: under the 227 KB per-block opt-in limit
+// with room for their few static words (the 1470-bit CRT takes 208 KB)
+constexpr int kRnsSmemCap = 224 * 1024;
 
 // per-L tables (device memory, filled by the host: blocksvibe_b200/rns.py)
 struct RnsTables {
@@ -896,7 +899,7 @@ int RnsLaunch<L>::split_mma(const RnsSplit& a, const RnsTables& tb, cudaStream_t
     static bool configured = false;
     const int smem = 128 * a.Ks + 2 * a.NS * a.Ks + tb.np * 512;
     if (!configured) {
-        int rc = (int)cudaFuncSetAttribute(k_rns_split_mma<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        int rc = (int)cudaFuncSetAttribute(k_rns_split_mma<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, kRnsSmemCap);
         if (rc) return rc;
         configured = true;
     }
@@ -919,7 +922,7 @@ int RnsLaunch<L>::crt_mma(const RnsCrt& a, const RnsTables& tb, cudaStream_t st)
     static bool configured = false;
     const int smem = (128 + 2 * a.NH) * a.Kc;
     if (!configured) {
-        int rc = (int)cudaFuncSetAttribute(k_rns_crt_mma<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        int rc = (int)cudaFuncSetAttribute(k_rns_crt_mma<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, kRnsSmemCap);
         if (rc) return rc;
         configured = true;
     }

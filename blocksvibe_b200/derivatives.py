@@ -31,6 +31,33 @@ from . import _lib, mpf, structure as S
 from .mpf import MPF
 
 
+def derivative_limbs(L, R, order):
+    """limbs of the derivative stages for recursion limbs L: the binomial sums of the stages (a_i[e] from the
+    moments, the polynomial part from D_i^w times moments) cancel terms up to about (2 order)^R larger than their
+    result, so where R log2(order) + 16 bits exceed the 62 bits by which L limbs exceed the task's precision, the
+    stages run with L + 4 limbs (128 more bits) and the results are rounded back to L limbs"""
+    guard = R * max(1.0, float(np.log2(max(order, 2)))) + 16
+    if guard <= 62 or MOMENTS != "staged":
+        return L
+    wide = L + 4
+    if not _lib.lib().b3d_supported_limbs(wide):
+        raise _lib.B3DError(f"no kernels compiled for the derivative stages' {wide} limbs")
+    return wide
+
+
+def resize(X, Lout):
+    """X with Lout limbs (L or L +- 4): widening exact, narrowing rounded once"""
+    if X.L == Lout:
+        return X
+    n = X.numel()
+    X = X.contiguous()
+    om = torch.empty((Lout,) + tuple(X.shape), dtype=torch.int32, device=X.device)
+    oe = torch.empty(tuple(X.shape), dtype=torch.int64, device=X.device)
+    _lib.call("b3d_resize", X.L, X.m.data_ptr(), X.e.data_ptr(), X.m.stride(0) if n else 0, n, Lout, om.data_ptr(),
+              oe.data_ptr(), om.stride(0) if n else 0, torch.cuda.current_stream(X.device).cuda_stream)
+    return MPF(om, oe)
+
+
 # Moments: "staged" (each level stages its terms, exact window sums flushed once per window: b3d_moments_stage /
 # b3d_moments_flush) or "per_level" (read-modify-write of every moment at every level: b3d_moments_level).
 MOMENTS = "staged"
@@ -115,8 +142,13 @@ class Derivs:
     """Post-recursion stages for one Plan and any batch of right-hand sides with lambda orders
     n >= Lambda - R.  two_js: internal spins to output (default: all two_j <= two_j_max)."""
 
-    def __init__(self, plan, R, L, two_js=None, kept_pole_order=None, device="cuda"):
+    def __init__(self, plan, R, L, two_js=None, kept_pole_order=None, device="cuda", Ld=None):
+        """L: limbs of the residues; Ld: limbs of the derivative stages and of the numerators they return
+        (default derivative_limbs(L, R, order))"""
         self.plan, self.R, self.L, self.device = plan, R, L, torch.device(device)
+        self.Ld = Ld if Ld is not None else derivative_limbs(L, R, plan.order)
+        if self.Ld not in (L, L + 4) or (self.Ld != L and MOMENTS != "staged"):
+            raise ValueError(f"derivative limbs {self.Ld} for residues of {L} limbs (L or L + 4, staged moments)")
         order = plan.order
         self.kept = kept_pole_order if kept_pole_order is not None and kept_pole_order < order else None
         tj12, tj43, tjmax = plan.tj12, plan.tj43, plan.tjmax
@@ -161,11 +193,11 @@ class Derivs:
 
     # ------------------------------------------------------------ constants (once per operator and R)
     def _constants(self):
-        L, R, order, Jo, NP, dev = self.L, self.R, self.plan.order, self.Jo, self.NP, self.device
+        L, R, order, Jo, NP, dev = self.Ld, self.R, self.plan.order, self.Jo, self.NP, self.device
         with mp.workprec(32 * L + 64):
             rc = 3 - 2 * mp.sqrt(2)
             pw = [rc ** n for n in range(order + 1)]
-            self.rcpow = mpf.from_mp(pw, L, (order + 1,), dev)
+            self.rcpow = mpf.from_mp(pw, self.L, (order + 1,), dev)       # the staged terms: residue limbs
             self.Wh = mpf.from_mp([(mp.mpf(n) ** k if (n or k) else 1) * pw[n] for k in range(R + 1) for n in range(order + 1)],
                                   L, (R + 1, order + 1), dev)
         # the shift of a polynomial in log r by a pole position D: T(D)[e][k] = C(e, k) D^(e - k), a Pascal matrix
@@ -223,12 +255,12 @@ class Derivs:
                 A[jo, :len(poly), i] = to_x(poly, npj - 1)
             for t, poly in enumerate(polys):
                 A[jo, :len(poly), NP + t] = to_x(poly, npj + t)
-        return mpf.from_fractions(list(A.reshape(-1)), self.L, (Jo, Dout, W), self.device)
+        return mpf.from_fractions(list(A.reshape(-1)), self.Ld, (Jo, Dout, W), self.device)
 
     def _small_constants(self):
         """R-dependent tables of the polynomial part: H[e][s] = sum_d C(e, d) G'[s][d] with
         G'[s][d] = G[s - 1 - d][d], P_e[t] = C(e, t) c[e - t] + H[e][e - t]"""
-        L, R, dev = self.L, self.R, self.device
+        L, R, dev = self.Ld, self.R, self.device
         R1 = R + 1
         self.Cb = mpf.from_ints([comb(e, d) for e in range(R1) for d in range(R1)], [0] * R1 * R1, L, (R1, R1), dev)
         Rw = max(R, 1)
@@ -269,8 +301,8 @@ class Derivs:
 
     def footprint_bytes(self, B):
         """device bytes of the moment accumulators (and the staging window) for B right-hand sides"""
-        per = (4 * self.L + 8) * 2 * self.Jo * self.NP * self.plan.Smax ** 2 * B
-        return per * (self.R + 1 + (self.stage_window(B) if MOMENTS == "staged" else 0))
+        per = 2 * self.Jo * self.NP * self.plan.Smax ** 2 * B
+        return per * ((4 * self.Ld + 8) * (self.R + 1) + (4 * self.L + 8) * (self.stage_window(B) if MOMENTS == "staged" else 0))
 
     # ------------------------------------------------------------ accumulation during the recursion
     def start(self, B):
@@ -278,7 +310,7 @@ class Derivs:
         self.B = B
         self.N = self.plan.Smax ** 2 * B
         rows = 2 * self.Jo * self.NP
-        self.mom = mpf.zeros((rows, self.R + 1, self.N), self.L, self.device)
+        self.mom = mpf.zeros((rows, self.R + 1, self.N), self.Ld, self.device)
         self._staged_mode = MOMENTS == "staged"
         if self._staged_mode:
             self._W = self.stage_window(B)
@@ -319,7 +351,7 @@ class Derivs:
         nkb = self._nkb[:R1].contiguous()
         _lib.call("b3d_moments_flush", self.L, p(self._stage.m), p(self._stage.e), self._stage.m.stride(0),
                   p(self._row_shift), self._m0, W, rows, self.N, R1, p(nk), p(nkb), self.plan.order + 1, self._KW,
-                  int(self._flushes > 0), p(self.mom.m), p(self.mom.e), self.mom.m.stride(0),
+                  int(self._flushes > 0), self.Ld, p(self.mom.m), p(self.mom.e), self.mom.m.stride(0),
                   torch.cuda.current_stream(self.device).cuda_stream)
         self._flushes += 1
         self._last = None
@@ -334,7 +366,8 @@ class Derivs:
     def finish_iter(self, h_inf, chunk=None):
         """as finish, by chunks of output spins: yields (first spin index, numerators)"""
         self.flush()
-        R, Jo, NP, order, L, dev = self.R, self.Jo, self.NP, self.plan.order, self.L, self.device
+        R, Jo, NP, order, L, dev = self.R, self.Jo, self.NP, self.plan.order, self.Ld, self.device
+        h_inf = resize(h_inf, L)
         R1, N, Rw = R + 1, self.N, max(R, 1)
         S2 = self.plan.Smax ** 2
         Nc = 2 * N

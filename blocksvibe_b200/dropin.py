@@ -30,7 +30,7 @@ import numpy as np
 import torch
 
 from . import mpf
-from .derivatives import Derivs
+from .derivatives import Derivs, resize
 from .mpf import MPF
 from .output import Output, apply_per_order
 from .plan import Plan
@@ -107,7 +107,7 @@ class Operator:
         self.rec = Recursion(self.plan, M, self.L, device=device)
         self.der = Derivs(self.plan, group.Lambda - parity, self.L, two_js=two_js,
                           kept_pole_order=group.kept_pole_order, device=device)
-        self.outs = {(c, d): Output(c, group.Lambda, parity, d, self.L, device) for c in coords for d in d12s}
+        self.outs = {(c, d): Output(c, group.Lambda, parity, d, self.der.Ld, device) for c in coords for d in d12s}
         self.device = torch.device(device)
 
     def footprint_bytes(self, B):
@@ -158,7 +158,8 @@ class Operator:
         return nums
 
     def apply_outputs(self, nums, d12):
-        return {c: apply_per_order(o, nums) for (c, dd), o in self.outs.items() if dd == d12}
+        """write_output of the numerators (derivative limbs), rounded to the task's L limbs"""
+        return {c: resize(apply_per_order(o, nums), self.L) for (c, dd), o in self.outs.items() if dd == d12}
 
     def to_host(self, outs):
         """device results -> host limb arrays through reusable pinned buffers (one D2H copy per array)"""

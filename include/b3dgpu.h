@@ -109,12 +109,19 @@ int b3d_moments_stage(int L, const int32_t* rm, const int64_t* re, int64_t rplan
                       int64_t yplane, void* stream);
 
 /* Flush a window of W staged levels: mom[(row * R1 + k) * N + c] = (mom +) round(sum_w n^k Y[w, row, c]) with
- * n = m0 + w + row_shift[row] (< NN), the sum exact above 2^-(32 L + 64) of its largest term, one rounding (and one
- * for the addition when accumulate != 0).  nk: n^k as KW 32-bit limbs, nk[(k * NN + n) * KW + j]; nkb[k * NN + n]
+ * n = m0 + w + row_shift[row] (< NN), the sum exact above 2^-(32 Lout + 64) of its largest term, one rounding (and one
+ * for the addition when accumulate != 0); Y has L limbs, the moments Lout = L or L + 4.  nk: n^k as KW 32-bit
+ * limbs, nk[(k * NN + n) * KW + j]; nkb[k * NN + n]
  * its bit length.  R1 <= 32, KW <= 12. */
 int b3d_moments_flush(int L, const int32_t* ym, const int64_t* ye, int64_t yplane, const int64_t* row_shift, int64_t m0,
                       int W, int64_t rows, int64_t N, int R1, const uint32_t* nk, const int32_t* nkb, int NN, int KW,
-                      int accumulate, int32_t* mm, int64_t* me, int64_t mplane, void* stream);
+                      int accumulate, int Lout, int32_t* mm, int64_t* me, int64_t mplane, void* stream);
+
+/* Change of limb count of n numbers, Lout = L or L +- 4: widening is exact, narrowing rounds once (half away from
+ * zero).  The derivative stages run with more limbs than the recursion where their sums cancel (the drop-in's
+ * choice; no counterpart in the reference, whose stages share one limb count). */
+int b3d_resize(int L, const int32_t* m, const int64_t* e, int64_t plane, int64_t n, int Lout, int32_t* om, int64_t* oe,
+               int64_t oplane, void* stream);
 
 /* ---- residue-number-system GEMM on the INT8 tensor cores (tcgen05), the replacement of the reference's
  * un-vendored sdpvibe mpf.gemm (RNS / INT8; called at recursion_gpu.py:53-79, derivatives.py:540-580,

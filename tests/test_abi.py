@@ -36,7 +36,7 @@ def test_library_exports_every_declared_symbol():
 def test_library_metadata_calls():
     lib = _lib.lib()
     assert lib.b3d_version() >= 100
-    for L in (6, 10, 18, 26, 30, 34, 42):
+    for L in (6, 10, 14, 18, 22, 26, 30, 34, 38, 42, 46):
         assert lib.b3d_supported_limbs(L) == 1
     assert lib.b3d_supported_limbs(7) == 0
 

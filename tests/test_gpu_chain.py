@@ -105,7 +105,7 @@ def test_staged_window_sums_cancel_exactly(cuda, monkeypatch):
     p = lambda t: t.data_ptr()
     from blocksvibe_b200 import _lib
     _lib.call("b3d_moments_flush", L, p(stage.m), p(stage.e), stage.m.stride(0), p(der._row_shift), 0, W, rows, N, R + 1,
-              p(der._nk[:R + 1].contiguous()), p(der._nkb[:R + 1].contiguous()), order + 1, der._KW, 0, p(mom.m),
+              p(der._nk[:R + 1].contiguous()), p(der._nkb[:R + 1].contiguous()), order + 1, der._KW, 0, L, p(mom.m),
               p(mom.e), mom.m.stride(0), torch.cuda.current_stream(cuda).cuda_stream)
     got = mpf.to_mp(mom)
     with mp.workprec(32 * L + 200):
@@ -153,3 +153,22 @@ def test_write_output_on_gpu(cuda, Lam, parity, D):
                        (o_rad, OO.xt_radial(num[0], Lam, parity, D))):
             got = list(mpf.to_mp(o.apply(X, nL=nL))[0, 0, 0, 0, :, 0])
             assert agreement_bits(got, ref) > 32 * L - 40
+
+
+@pytest.mark.parametrize("L", [10, 34, 42])
+def test_resize_widens_exactly_and_narrows_once(cuda, L):
+    """b3d_resize: L -> L + 4 keeps every value, L + 4 -> L rounds once as the host conversions round"""
+    g = torch.Generator().manual_seed(L)
+    X = mpf.random_mpf((300,), L, spread=30, device=cuda, generator=g)
+    X.m[:, 0] = 0
+    X.e[0] = mpf.EZ
+    W = DV.resize(X, L + 4)
+    assert W.L == L + 4
+    assert list(mpf.to_mp(W)) == list(mpf.to_mp(X))
+    back = DV.resize(W, L)
+    assert torch.equal(back.m, X.m) and torch.equal(back.e, X.e)
+    Y = mpf.random_mpf((300,), L + 4, spread=30, device=cuda, generator=g)
+    got = mpf.to_mp(DV.resize(Y, L))
+    with mp.workprec(32 * (L + 4) + 64):
+        want = mpf.to_mp(mpf.from_mp(list(mpf.to_mp(Y)), L))
+    assert list(got) == list(want)

@@ -13,7 +13,7 @@ import pytest
 
 from blocksvibe_b200 import rns
 
-LIMBS = (6, 10, 18, 26, 30, 34, 42)
+LIMBS = (6, 10, 14, 18, 22, 26, 30, 34, 38, 42, 46)
 KMAX = 4096
 
 
