@@ -48,6 +48,9 @@ def parse():
     ap.add_argument("--moments", default=None, choices=(None, "staged", "per_level"), help="moments form")
     ap.add_argument("--no-set644", action="store_true", help="default run: skip the full 644-task set")
     ap.add_argument("--no-cfg4", action="store_true", help="default run: skip the serving stream at its stated rate")
+    ap.add_argument("--one-step", action="store_true",
+                    help="run one launched step and one JSON render of the workload, untimed, and exit (the case "
+                         "that kernel profiles capture; with --schedule plain each recursion has one right-hand side)")
     return ap.parse_args()
 
 
@@ -355,6 +358,19 @@ def run_ours(args):
     dtask = DI.Task(t.q4, t.sign, t.pp, t.two_js_internal, t.coordinates, t.delta_1_plus_2,
                     {n: MPF(h.m.to(dev), h.e.to(dev)) for n, h in t.h_inf.items()})
     run = op.run_batched if args.schedule == "batched" else op.run_plain
+    if args.one_step:
+        from blocksvibe_b200 import jsonout as JO
+        probe = Probe()
+        outs = op.apply_outputs(run([dtask], ns), t.delta_1_plus_2)
+        outputs = {cc: list(o.outputs) for (cc, d), o in op.outs.items() if d == t.delta_1_plus_2}
+        x0 = next(iter(outs.values()))
+        w = JO.SpinWriter(JO.task_options(G, t), sorted(t.two_js_internal), t.pp, outputs, op.plan.Smax, 1,
+                          x0.shape[-1], dev)
+        w.render_device(outs, 0)
+        torch.cuda.synchronize()
+        print(json.dumps({"one_step": args.workload, "schedule": args.schedule, "launches": probe.launches,
+                          "peak_device_bytes": torch.cuda.max_memory_allocated(dev)}), flush=True)
+        return
     graph = None
     if args.schedule == "batched" and not args.no_graph:
         graph = DI.GraphStep(op, 1, ns, t.delta_1_plus_2)

@@ -13,8 +13,10 @@ conformal_block_derivatives, restore_r_delta, shift_block, together_with_factors
   P_e[t]  = C(e, t) c[e-t] + sum_{u=t+1}^{e} C(e, u) G[e-u][u-t-1]
   num_e(x) = P_e(x + ub) Pi(x) + sum_i a_i[e] Pi_i(x),   Pi = prod_i (x - x_i),  Pi_i = Pi / (x - x_i)
 
-The moments v are accumulated during the recursion (one kernel per level, libb3dgpu b3d_moments_level);
-c, a, G, the polynomial part and the numerators are multiprecision GEMMs.  The numerator matrix
+The moments v are accumulated during the recursion: each level's terms res r_c^n are staged
+(b3d_moments_stage) and the moments of a window of levels are formed once (b3d_moments_flush; the
+per-level read-modify-write form b3d_moments_level is kept as MOMENTS = "per_level"); c, a, G, the polynomial
+part and the numerators are multiprecision GEMMs, at derivative_limbs(L, R, order) limbs.  The numerator matrix
 A_j = [Pi_i(x) | Pi(x) (x + ub)^t] is exact: in y = 2x the roots are integers.  Pole shifting
 (kept_pole_order < order) replaces the unprotected poles by the kept ones (blocks_3d's shift_poles); the
 replaced pole's column has the closed form of numerator_basis_y, exact in rationals and folded into the
