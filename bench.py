@@ -45,6 +45,7 @@ def parse():
     ap.add_argument("--rate", type=float, default=200.0, help="cfg4: Poisson arrival rate (tasks/s)")
     ap.add_argument("--requests", type=int, default=32, help="cfg4: requests in the stream")
     ap.add_argument("--cauchy", default=None, help="Cauchy kernel form (Recursion's cauchy argument)")
+    ap.add_argument("--pole", default=None, choices=(None, "mma", "cuda"), help="pole-step kernel form")
     ap.add_argument("--moments", default=None, choices=(None, "staged", "per_level"), help="moments form")
     ap.add_argument("--no-set644", action="store_true", help="default run: skip the full 644-task set")
     ap.add_argument("--no-cfg4", action="store_true", help="default run: skip the serving stream at its stated rate")
@@ -151,7 +152,7 @@ class Clocks:
 
 
 # ---------------------------------------------------------------- kernel probe (launch count, per-kernel events)
-KERNELS_PER_CALL = {"b3d_pole_level": 2, "b3d_cauchy_align": 2, "b3d_cauchy_align_sm": 2}
+KERNELS_PER_CALL = {"b3d_pole_level": 2, "b3d_pole_level_mma": 2, "b3d_cauchy_align": 2, "b3d_cauchy_align_sm": 2}
 
 
 class Probe:
@@ -765,6 +766,8 @@ def main():
     from blocksvibe_b200 import derivatives as DV, recursion as RC
     if args.cauchy:
         RC.CAUCHY = args.cauchy
+    if args.pole:
+        RC.POLE = args.pole
     if args.moments:
         DV.MOMENTS = args.moments
     if args.impl == "reference":

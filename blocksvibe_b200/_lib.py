@@ -20,6 +20,8 @@ SIGNATURES = {
     "b3d_add": [_I, _P, _P, _Q, _P, _P, _P, _Q, _P, _Q, _P, _P, _Q, _P],
     "b3d_cauchy_level": [_I, _P, _P, _Q, _P, _P, _Q, _P, _P, _P, _Q, _P],
     "b3d_pole_level": [_I, _P, _P, _Q, _P, _P, _Q, _P, _P, _Q, _P, _P, _P, _P, _Q, _Q, _I, _P, _P, _Q, _P, _P, _Q, _P],
+    "b3d_pole_level_mma": [_I, _P, _P, _Q, _P, _P, _Q, _P, _P, _Q, _P, _P, _P, _P, _Q, _Q, _I, _P, _P, _Q, _P, _P, _Q,
+                           _P, _P],
     "b3d_moments_level": [_I, _P, _P, _Q, _P, _P, _Q, _P, _P, _P, _Q, _Q, _I, _P, _P, _Q, _P],
     "b3d_moments_stage": [_I, _P, _P, _Q, _P, _P, _Q, _P, _P, _P, _Q, _Q, _Q, _Q, _P, _P, _Q, _P],
     "b3d_moments_flush": [_I, _P, _P, _Q, _P, _Q, _I, _Q, _Q, _I, _P, _P, _I, _I, _I, _I, _P, _P, _Q, _P],

@@ -100,6 +100,19 @@ int b3d_pole_level(int L, const int32_t* hm, const int64_t* he, int64_t hplane, 
                                 "b3d_pole_level"));
 }
 
+int b3d_pole_level_mma(int L, const int32_t* hm, const int64_t* he, int64_t hplane, const int32_t* Rm,
+                       const int64_t* Re, int64_t Rplane, const int32_t* Qm, const int64_t* Qe, int64_t Qplane,
+                       const int64_t* t_hrow, const int64_t* t_R, const int64_t* t_qL, const int64_t* t_slot,
+                       int64_t T, int64_t B, int S, int32_t* ym, int64_t* ye, int64_t yplane, int32_t* rm,
+                       int64_t* re, int64_t rplane, int* err, void* stream) {
+    if (!nonneg(T) || B < 1 || S < 1) return fail(B3D_E_ARG, "b3d_pole_level_mma: invalid size");
+    if (S > 8) return fail(B3D_E_ARG, "b3d_pole_level_mma: S > 8 (use b3d_pole_level)");
+    if (!err) return fail(B3D_E_ARG, "b3d_pole_level_mma: no error flag");
+    B3D_DISPATCH(L, cuda_status(LX::pole_mma(hm, he, hplane, Rm, Re, Rplane, Qm, Qe, Qplane, t_hrow, t_R, t_qL, t_slot,
+                                            T, B, S, ym, ye, yplane, rm, re, rplane, err, as_stream(stream)),
+                                "b3d_pole_level_mma"));
+}
+
 int b3d_moments_level(int L, const int32_t* rm, const int64_t* re, int64_t rplane, const int32_t* pm,
                       const int64_t* pe, int64_t pplane, const int64_t* q_slot, const int64_t* q_row,
                       const int64_t* q_n, int64_t Q, int64_t N, int R1, int32_t* mm, int64_t* me, int64_t mplane,

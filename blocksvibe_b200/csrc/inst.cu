@@ -4,6 +4,7 @@
 #include "rns.cuh"
 #include "cauchy_rns.cuh"
 #include "decimal.cuh"
+#include "pole_mma.cuh"
 
 #ifndef B3D_L
 #error "compile with -DB3D_L=<limbs>"

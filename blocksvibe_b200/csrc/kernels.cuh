@@ -1006,6 +1006,11 @@ struct Launch {
                     const int32_t* Qm, const i64* Qe, i64 Qplane, const i64* t_hrow, const i64* t_R, const i64* t_qL,
                     const i64* t_slot, i64 T, i64 B, int S, int32_t* ym, i64* ye, i64 yplane,
                     int32_t* rm, i64* re, i64 rplane, cudaStream_t st);
+    // the same pole step on the tensor cores (pole_mma.cuh); err: device flag of bounded-wait expiries
+    static int pole_mma(const int32_t* hm, const i64* he, i64 hplane, const int32_t* Rm, const i64* Re, i64 Rplane,
+                        const int32_t* Qm, const i64* Qe, i64 Qplane, const i64* t_hrow, const i64* t_R, const i64* t_qL,
+                        const i64* t_slot, i64 T, i64 B, int S, int32_t* ym, i64* ye, i64 yplane,
+                        int32_t* rm, i64* re, i64 rplane, int* err, cudaStream_t st);
     static int moments(const int32_t* rm, const i64* re, i64 rplane, const int32_t* pm, const i64* pe, i64 pplane,
                        const i64* q_slot, const i64* q_row, const i64* q_n, i64 Q, i64 N, int R1,
                        int32_t* mm, i64* me, i64 mplane, cudaStream_t st);

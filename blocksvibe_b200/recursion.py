@@ -4,7 +4,8 @@ contract.
 
 Per level m (a ``Plan`` level): one kernel for the Cauchy step fused with the h_inf term
 (``b3d_cauchy_level``), one pair of kernels for the pole step writing straight into the slot buffer
-(``b3d_pole_level``), then the caller's hook (the derivative moments).  Constants are built once per
+(``b3d_pole_level_mma``: the exact sums as INT8 tensor-core GEMMs of base-256 digits; ``b3d_pole_level``: the
+same bits on the CUDA cores), then the caller's hook (the derivative moments).  Constants are built once per
 operator: the M-matrix table, the exact Q values with their sign, q L for every (L, Q) pair of the plan,
 and the R and q L tables aligned per row for the pole step.
 """
@@ -17,8 +18,9 @@ from . import _lib, mpf, structure as S
 from .mpf import MPF
 
 
-# default Cauchy kernel (see Recursion)
+# default Cauchy kernel and pole-step kernel (see Recursion)
 CAUCHY = "cuda4"
+POLE = "mma"
 
 
 def _dev(a, device):
@@ -29,14 +31,20 @@ class Recursion:
     """Numbers of one Plan on the GPU.  M: dict key -> matrix of decimal strings (keys as plan.Mkeys),
     an MPF table (nM, Smax, Smax) in plan.Mkeys order, or None for random O(1) matrices (timing runs)."""
 
-    def __init__(self, plan, M, L, device="cuda", generator=None, cauchy=None, rns_min_k=32):
+    def __init__(self, plan, M, L, device="cuda", generator=None, cauchy=None, rns_min_k=32, pole=None):
         """cauchy: "cuda" (one-limb divisions on the CUDA cores, b3d_cauchy_level), "cuda2" (the same quotients from
         pre-aligned columns, two per thread, b3d_cauchy_align + b3d_cauchy_level2: bit-identical to "cuda"), "cuda3"
         (cuda2 with 24- or 22-bit quotient digits when the plan's divisors allow, b3d_cauchy_level3: bit-identical), "cuda4"
         (cuda3 on sign-magnitude columns read limb by limb, b3d_cauchy_align_sm + b3d_cauchy_level4: bit-identical), "rns"
         (the level's Cauchy GEMM on the tensor cores, residues + CRT), or "auto" (rns for levels with at least
-        rns_min_k columns, cuda2 below)"""
+        rns_min_k columns, cuda2 below).  pole: "mma" (the pole step's exact sums on the INT8 tensor cores,
+        b3d_pole_level_mma; plans with Smax <= 8) or "cuda" (b3d_pole_level): bit-identical"""
         self.cauchy, self.rns_min_k = cauchy or CAUCHY, rns_min_k
+        self.pole = pole or POLE
+        if self.pole not in ("mma", "cuda"):
+            raise ValueError(f"pole must be 'mma' or 'cuda', not {self.pole!r}")
+        if self.pole == "mma" and plan.Smax > 8:
+            self.pole = "cuda"
         self._side = {}                                  # calling stream -> stream of the per-level hook
         self.overlap_hook = True
         if not _lib.lib().b3d_supported_limbs(L):
@@ -44,6 +52,7 @@ class Recursion:
         if plan.dmax >= 1 << 16:
             raise _lib.B3DError(f"Cauchy differences up to {plan.dmax} exceed the one-limb kernel (< 65536)")
         self.plan, self.L, self.device = plan, L, torch.device(device)
+        self.err = torch.zeros(1, dtype=torch.int32, device=self.device)   # bounded-wait expiries of the kernels
         Sm, nM = plan.Smax, len(plan.Mkeys)
         if M is None:
             self.Mtab = mpf.random_mpf((nM, Sm, Sm), L, spread=1, device=self.device, generator=generator)
@@ -219,11 +228,15 @@ class Recursion:
             if pending is not None:                      # slots written below may still be read by the hook
                 main.wait_event(pending)
                 pending = None
-            _lib.call("b3d_pole_level", L, p(H.m), p(H.e), H.m.stride(0),
-                      p(self.Ralign[0]), p(self.Ralign[1]), self.Ralign[0].stride(0),
-                      p(self.QLalign[0]), p(self.QLalign[1]), self.QLalign[0].stride(0),
-                      p(lev["t_hrow"]), p(lev["t_R"]), p(lev["t_qL"]), p(lev["t_slot"]), lev["T"], B, Sm,
-                      p(Y.m), p(Y.e), Y.m.stride(0), p(res.m), p(res.e), res.m.stride(0), stream)
+            pole_args = (L, p(H.m), p(H.e), H.m.stride(0),
+                         p(self.Ralign[0]), p(self.Ralign[1]), self.Ralign[0].stride(0),
+                         p(self.QLalign[0]), p(self.QLalign[1]), self.QLalign[0].stride(0),
+                         p(lev["t_hrow"]), p(lev["t_R"]), p(lev["t_qL"]), p(lev["t_slot"]), lev["T"], B, Sm,
+                         p(Y.m), p(Y.e), Y.m.stride(0), p(res.m), p(res.e), res.m.stride(0))
+            if self.pole == "mma":
+                _lib.call("b3d_pole_level_mma", *pole_args, p(self.err), stream)
+            else:
+                _lib.call("b3d_pole_level", *pole_args, stream)
             if hook is not None and side is not None:
                 ready = torch.cuda.Event()
                 ready.record(main)
@@ -237,6 +250,13 @@ class Recursion:
         if pending is not None:
             main.wait_event(pending)
         return res
+
+    def check_errors(self):
+        """raise B3DError if a kernel of this recursion gave up a bounded wait (synchronises the device)"""
+        code = int(self.err.item())
+        if code:
+            self.err.zero_()
+            raise _lib.B3DError(f"pole step: a bounded wait of the tensor-core kernel expired (code {code})")
 
     def slot(self, p, m, jidx, pidx):
         """physical slot of residue (p, m, jidx, pidx) (meaningful after run() only without slot reuse)"""

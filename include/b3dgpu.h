@@ -91,6 +91,17 @@ int b3d_pole_level(int L, const int32_t* hm, const int64_t* he, int64_t hplane, 
                    int64_t T, int64_t B, int S, int32_t* ym, int64_t* ye, int64_t yplane, int32_t* rm,
                    int64_t* re, int64_t rplane, void* stream);
 
+/* The same pole step with its exact sums on the INT8 tensor cores (replaces Recursion._pole with
+ * pole="gemm", recursion_gpu.py:494-498, and the small GEMMs of smallgemm.py:18-88): per task and row of the
+ * constant, one tcgen05 GEMM of balanced base-256 digits (a Hankel matrix of the constant's digits against the
+ * reversed digits of the aligned columns), carry chain and one rounding; bit-identical to b3d_pole_level.
+ * S <= 8.  err: a device int set nonzero if a bounded wait of the kernel expired (results then incomplete). */
+int b3d_pole_level_mma(int L, const int32_t* hm, const int64_t* he, int64_t hplane, const int32_t* Rm,
+                       const int64_t* Re, int64_t Rplane, const int32_t* Qm, const int64_t* Qe, int64_t Qplane,
+                       const int64_t* t_hrow, const int64_t* t_R, const int64_t* t_qL, const int64_t* t_slot,
+                       int64_t T, int64_t B, int S, int32_t* ym, int64_t* ye, int64_t yplane, int32_t* rm,
+                       int64_t* re, int64_t rplane, int* err, void* stream);
+
 /* Derivative moments of one recursion level (replaces Derivs.accumulate + momacc, derivatives.py:48-96,
  * :486-510): for each entry q and column c, y = res[q_slot[q], c] * rcpow[q_n[q]] and
  * mom[q_row[q], k, c] += q_n[q]^k y for k < R1.  res: (nslots, N), rcpow: (order + 1), mom: (rows, R1, N). */

@@ -129,3 +129,25 @@ def test_cauchy_forms_bitwise_equal(cuda, case):
         outs.append(rec.run(hinf_tensor(H, plan, order, nrhs, L, cuda)))
     for o in outs[1:]:
         assert torch.equal(outs[0].m, o.m) and torch.equal(outs[0].e, o.e)
+
+
+@pytest.mark.parametrize("case", [
+    (4, 2, 6, 9, ((0, 1), (1, 0)), 10, 3, 71),
+    (8, 8, 6, 8, ((0, 0), (1, 1)), 34, 2, 72),
+    (4, 4, 8, 8, ((0, 0), (1, 1)), 26, 5, 73),
+    (8, 8, 6, 6, ((0, 1), (1, 0)), 42, 3, 74),
+    (8, 8, 4, 6, ((0, 0), (1, 1)), 46, 14, 75),             # S B = 70 columns: two column chunks
+])
+def test_pole_forms_bitwise_equal(cuda, case):
+    """the pole step's exact sums on the tensor cores (b3d_pole_level_mma) give the CUDA-core kernels' bits
+    over a whole recursion with slot recycling, and the residues meet the oracle's bar"""
+    tj12, tj43, tjmax, order, pp, L, nrhs, seed = case
+    M, H = random_case(*case)
+    plan = PL.Plan(tj12, tj43, tjmax, order, pp, reuse=True)
+    outs = []
+    for form in ("cuda", "mma"):
+        rec = RC.Recursion(plan, M, L, device=cuda, pole=form)
+        outs.append(rec.run(hinf_tensor(H, plan, order, nrhs, L, cuda)))
+        rec.check_errors()
+    assert torch.equal(outs[0].m, outs[1].m) and torch.equal(outs[0].e, outs[1].e)
+    check(tj12, tj43, tjmax, order, pp, L, nrhs, M, H, cuda)
