@@ -45,7 +45,7 @@ def parse():
     ap.add_argument("--rate", type=float, default=200.0, help="cfg4: Poisson arrival rate (tasks/s)")
     ap.add_argument("--requests", type=int, default=32, help="cfg4: requests in the stream")
     ap.add_argument("--cauchy", default=None, help="Cauchy kernel form (Recursion's cauchy argument)")
-    ap.add_argument("--pole", default=None, choices=(None, "mma", "cuda"), help="pole-step kernel form")
+    ap.add_argument("--pole", default=None, choices=(None, "auto", "mma", "cuda"), help="pole-step kernel form")
     ap.add_argument("--moments", default=None, choices=(None, "staged", "per_level"), help="moments form")
     ap.add_argument("--no-set644", action="store_true", help="default run: skip the full 644-task set")
     ap.add_argument("--no-cfg4", action="store_true", help="default run: skip the serving stream at its stated rate")
@@ -194,7 +194,16 @@ def peaks():
     return 6650.0, "fallback"
 
 
+_INT8_PEAK = {}
+
+
 def int8_peak_tops(device):
+    if str(device) not in _INT8_PEAK:
+        _INT8_PEAK[str(device)] = _int8_peak_tops(device)
+    return _INT8_PEAK[str(device)]
+
+
+def _int8_peak_tops(device):
     """dense INT8 tensor throughput of this GPU, measured with a plain library GEMM (torch._int_mm on 8192^3,
     best of 5): the denominator of the RNS GEMM's tensor roofline (no INT8 figure is in MEASURED_PEAKS.json)"""
     import torch
@@ -493,7 +502,7 @@ def run_ours(args):
     if dominant in ("b3d_cauchy_level", "b3d_cauchy_level2", "b3d_cauchy_level3", "b3d_cauchy_level4"):
         per_step_bytes = sum(RL.cauchy_level_bytes(lv, N, L) for lv in levs if lv["m"] > 0 or dominant == "b3d_cauchy_level") \
             * (1 if args.schedule == "batched" else len(ns))
-    elif dominant == "b3d_pole_level":
+    elif dominant in ("b3d_pole_level", "b3d_pole_level_mma"):
         per_step_bytes = sum(RL.pole_level_bytes(lv, N, S, L) for lv in levs) * (1 if args.schedule == "batched" else len(ns))
     else:
         per_step_bytes = None
@@ -521,6 +530,21 @@ def run_ours(args):
                        "issued_over_algorithmic": RNS.MMA_STATS["macs"] / RNS.MMA_STATS["alg_macs"],
                        "launches_per_step": len(RNS.MMA_TIMER), "ms_per_step": mma_s * 1e3}
     RNS.MMA_TIMER = None
+    # tensor roofline of the pole step when it runs on the tensor cores: int8 MACs issued by its MMAs per step
+    # over its CUDA-event time per step (split), with the share of those MACs the exact sums need
+    pole_roof = None
+    if "b3d_pole_level_mma" in split:
+        issued = useful = 0
+        for lv in levs:
+            i_, u_ = RL.pole_mma_macs(lv, N, S, L)
+            issued, useful = issued + i_, useful + u_
+        reps = 1 if args.schedule == "batched" else len(ns)
+        pole_s = split["b3d_pole_level_mma"] / 1e3
+        peak8 = int8_peak_tops(dev)
+        ach = 2 * issued * reps / pole_s / 1e12
+        pole_roof = {"kernel": "k_pole_mma (tcgen05.mma.kind::i8)", "bound": "tensor", "achieved": ach, "peak": peak8,
+                     "unit": "TOPS", "frac": ach / peak8, "peak_source": "measured here: torch._int_mm 8192^3",
+                     "issued_over_algorithmic": issued / useful, "ms_per_step": pole_s * 1e3}
     if rank != 0:
         if world > 1:
             import torch.distributed as dist
@@ -552,7 +576,7 @@ def run_ours(args):
             "e2e_with_json": {"value": world / (e2e_s + jout["e2e_ms"] / 1e3), "unit": "tasks/s",
                               "what": "e2e plus the task's blocks_3d JSON files formatted on the GPU and copied to "
                                       "pinned host memory (the files blocks_3d writes)"},
-            "roofline": roof, "tensor_roofline": tensor_roof, "json_output": jout, "cpu_baseline": cpu, "clocks": clk,
+            "roofline": roof, "tensor_roofline": tensor_roof, "pole_tensor_roofline": pole_roof, "json_output": jout, "cpu_baseline": cpu, "clocks": clk,
             "set644": set644, "cfg4": cfg4}
     print(json.dumps(line), flush=True)
     if world > 1:

@@ -20,7 +20,25 @@ from .mpf import MPF
 
 # default Cauchy kernel and pole-step kernel (see Recursion)
 CAUCHY = "cuda4"
-POLE = "mma"
+POLE = "auto"
+# Which pole-step form is faster.  The tensor-core form takes a task's S B columns in chunks of 32 at a cost per
+# chunk that hardly depends on how many columns are in use; the CUDA-core form costs in proportion to the
+# columns.  Measured on a B200 (both forms, both stages, 3000 synthetic tasks per shape, L in {26, 30, 34, 42},
+# S in {2 .. 5}, S B from 5 to 130): the time ratio CUDA cores / tensor cores of a full chunk, by (L, S); for other
+# column counts the ratio scales with the chunks' fill (S B / (32 chunks)) to within a few percent.
+POLE_FULL_CHUNK_RATIO = {26: (0.71, 0.91, 1.09, 1.23), 30: (0.64, 0.85, 1.02, 1.14), 34: (0.73, 0.93, 1.09, 1.24),
+                         42: (0.90, 1.15, 1.32, 1.51)}            # S = 2, 3, 4, 5
+POLE_MIN_GAIN = 1.05
+
+
+def pole_mma_gain(L, S, B):
+    """predicted time ratio CUDA-core / tensor-core pole step (above 1: the tensor cores are faster)"""
+    if S < 2:
+        return 0.0
+    Lk = max((k for k in POLE_FULL_CHUNK_RATIO if k <= L), default=26)
+    r = POLE_FULL_CHUNK_RATIO[Lk][min(S, 5) - 2]
+    cols = S * B
+    return r * cols / (32 * -(-cols // 32))
 
 
 def _dev(a, device):
@@ -38,12 +56,13 @@ class Recursion:
         (cuda3 on sign-magnitude columns read limb by limb, b3d_cauchy_align_sm + b3d_cauchy_level4: bit-identical), "rns"
         (the level's Cauchy GEMM on the tensor cores, residues + CRT), or "auto" (rns for levels with at least
         rns_min_k columns, cuda2 below).  pole: "mma" (the pole step's exact sums on the INT8 tensor cores,
-        b3d_pole_level_mma; plans with Smax <= 8) or "cuda" (b3d_pole_level): bit-identical"""
+        b3d_pole_level_mma; plans with Smax <= 8), "cuda" (b3d_pole_level) or "auto" (mma where the measured
+        crossover, pole_mma_gain, predicts it faster, cuda elsewhere): bit-identical"""
         self.cauchy, self.rns_min_k = cauchy or CAUCHY, rns_min_k
         self.pole = pole or POLE
-        if self.pole not in ("mma", "cuda"):
-            raise ValueError(f"pole must be 'mma' or 'cuda', not {self.pole!r}")
-        if self.pole == "mma" and plan.Smax > 8:
+        if self.pole not in ("mma", "cuda", "auto"):
+            raise ValueError(f"pole must be 'mma', 'cuda' or 'auto', not {self.pole!r}")
+        if self.pole != "cuda" and plan.Smax > 8:
             self.pole = "cuda"
         self._side = {}                                  # calling stream -> stream of the per-level hook
         self.overlap_hook = True
@@ -193,6 +212,7 @@ class Recursion:
             if side is None:
                 side = self._side[stream] = torch.cuda.Stream(dev)
         pending = None                                   # the side stream's last hook, not yet joined
+        use_mma = self.uses_mma(B)
         p = lambda t: t.data_ptr()
         for lev in self.levels:
             if lev is None:
@@ -233,7 +253,7 @@ class Recursion:
                          p(self.QLalign[0]), p(self.QLalign[1]), self.QLalign[0].stride(0),
                          p(lev["t_hrow"]), p(lev["t_R"]), p(lev["t_qL"]), p(lev["t_slot"]), lev["T"], B, Sm,
                          p(Y.m), p(Y.e), Y.m.stride(0), p(res.m), p(res.e), res.m.stride(0))
-            if self.pole == "mma":
+            if use_mma:
                 _lib.call("b3d_pole_level_mma", *pole_args, p(self.err), stream)
             else:
                 _lib.call("b3d_pole_level", *pole_args, stream)
@@ -250,6 +270,12 @@ class Recursion:
         if pending is not None:
             main.wait_event(pending)
         return res
+
+    def uses_mma(self, B):
+        """whether run() with B right-hand sides takes the tensor-core pole step"""
+        if self.pole != "auto":
+            return self.pole == "mma"
+        return pole_mma_gain(self.L, self.plan.Smax, B) >= POLE_MIN_GAIN
 
     def check_errors(self):
         """raise B3DError if a kernel of this recursion gave up a bounded wait (synchronises the device)"""

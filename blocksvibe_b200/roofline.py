@@ -28,3 +28,27 @@ def cauchy_level_macs(lev, N):
 
 def pole_level_macs(lev, N, S):
     return len(lev["t_slot"]) * 2 * S * N
+
+
+def pole_mma_geometry(L):
+    """(U, MT): digits per entry along K and 128-position tiles of the tensor-core pole step (pole_mma.cuh)"""
+    NB, D = 32 * L - 2, 4 * L
+    U = 32 * (-(-D // 32))
+
+    def p0(mt):
+        top = 8 * L - 1 - 128 * mt
+        return 0 if top <= 0 else 16 * (-(-top // 16))
+    return U, (1 if 8 * p0(1) + 17 <= NB - 160 else 2)
+
+
+def pole_mma_macs(lev, N, S, L):
+    """int8 MACs of both stages of b3d_pole_level_mma on one level: (issued by the MMAs, digit products of the
+    exact sums).  Per task and stage: S rows x S entries x U / 32 K steps x MT tiles of 128 x NC x 32 MACs per
+    column chunk; the exact sums need S^2 N (4 L)^2 digit products."""
+    U, MT = pole_mma_geometry(L)
+    T = len(lev["t_slot"])
+    nc = 32 if N >= 32 else 16 * (-(-N // 16))
+    chunks = -(-N // nc)
+    issued = 2 * T * chunks * S * S * (U // 32) * MT * 128 * nc * 32
+    useful = 2 * T * S * S * N * (4 * L) ** 2
+    return issued, useful
