@@ -273,6 +273,34 @@ __device__ __forceinline__ u32 pm_limb(const PmHead& h, const u32* col, int st, 
     return k < h.kz ? 0u : (k == h.kz ? 0u - r : ~r);
 }
 
+// limbs [w KQ, (w + 1) KQ) of the stored result (KQ = ceil(L / 4)), written to out[k * plane]: the KQ + 1
+// magnitude limbs they read are loaded once
+template <int L, int NW>
+__device__ __forceinline__ void pm_limbs(const PmHead& h, const u32* col, int st, int w, int32_t* out, i64 plane) {
+    constexpr int NB = nb_bits(L), KQ = (L + 3) / 4;
+    const int k0 = w * KQ;
+    if (h.mode != PmHead::kLimbs) {
+#pragma unroll
+        for (int q = 0; q < KQ; q++) {
+            const int k = k0 + q;
+            if (k < L) out[k * plane] = (int32_t)pm_limb<L, NW>(h, col, st, k);
+        }
+        return;
+    }
+    u32 mm[KQ + 1];
+#pragma unroll
+    for (int q = 0; q <= KQ; q++) mm[q] = pm_mag<NW>(col, st, h.Q + k0 + q, h.neg, h.z);
+#pragma unroll
+    for (int q = 0; q < KQ; q++) {
+        const int k = k0 + q;
+        if (k < L) {
+            const u32 r = fsr(mm[q], mm[q + 1], h.F) + (k <= h.kc ? 1u : 0u);
+            out[k * plane] = (int32_t)(!h.neg ? r : (k < h.kz ? 0u : (k == h.kz ? 0u - r : ~r)));
+        }
+    }
+    (void)NB;
+}
+
 // col (two's complement limbs, stride st) += sum_{p < P0} D[p, n] 256^p, from the digits in shared memory
 // (the rare exact redo)
 template <int L>
@@ -380,9 +408,9 @@ __global__ void __launch_bounds__(kPoleMmaThreads, 3) k_pole_mma(PoleMmaArgs a) 
             pm_put_digits<L>(cn, cneg, cdig + lane * CW + G::PADB / 4);
             if (S > 1) cneg = load_mag<L>(a.cm, a.cplane, (crow * S + 1) * S + lane, cn);
         }
-        // column exponents: the largest over j of the nonzero entries (all loads of a column issued at once)
         const i64 xbase = xrow * S * S * a.B, obase = orow * S * S * a.B;
         const int jst = pm_jst(a);
+        // column exponents: the largest over j of the nonzero entries (all loads of a column issued at once)
         for (int n = tid; n < NC; n += blockDim.x) {
             i64 E = EZ;
             const int co = n < nn ? pm_coff(a, (int)n0 + n) : 0;
@@ -558,17 +586,33 @@ __global__ void __launch_bounds__(kPoleMmaThreads, 3) k_pole_mma(PoleMmaArgs a) 
                     const i64 E = ecol[n];
                     if (E != EZ) {
                         u32* col = accs + n;
-                        i64 C = carr[0][n];
-#pragma unroll 1
-                        for (int sg = 1; sg < 4 * MT; sg++) {
-                            const int kend = P0 / 4 + 8 * (sg + 1) < NW ? P0 / 4 + 8 * (sg + 1) : NW;
-                            for (int k = P0 / 4 + 8 * sg; C != 0 && k < kend; k++) {
-                                const i64 v = (i64)col[k * ast] + C;
+                        // segment sg (sg >= 1) receives the carry out of segment sg - 1 (all segments at once);
+                        // what then runs out of the top of a segment (rare) is passed on in order afterwards
+                        constexpr int NSEG = 4 * MT;
+                        i64 e[NSEG];
+#pragma unroll
+                        for (int sg = 0; sg < NSEG; sg++) {
+                            i64 c = sg > 0 ? carr[sg - 1][n] : 0;
+                            const int k0 = P0 / 4 + 8 * sg, kend = k0 + 8 < NW ? k0 + 8 : NW;
+                            for (int k = k0; c != 0 && k < kend; k++) {
+                                const i64 v = (i64)col[k * ast] + c;
                                 col[k * ast] = (u32)v;
-                                C = v >> 32;
+                                c = v >> 32;
                             }
-                            C += carr[sg][n];
+                            e[sg] = c;
                         }
+                        i64 x = 0;
+#pragma unroll
+                        for (int sg = 1; sg < NSEG; sg++) {
+                            x += e[sg - 1];
+                            const int k0 = P0 / 4 + 8 * sg, kend = k0 + 8 < NW ? k0 + 8 : NW;
+                            for (int k = k0; x != 0 && k < kend; k++) {
+                                const i64 v = (i64)col[k * ast] + x;
+                                col[k * ast] = (u32)v;
+                                x = v >> 32;
+                            }
+                        }
+                        i64 C = carr[NSEG - 1][n] + x + e[NSEG - 1];
                         for (int k = P0 / 4 + VW; k < NW; k++) {
                             col[k * ast] = (u32)C;
                             C >>= 32;
@@ -598,13 +642,12 @@ __global__ void __launch_bounds__(kPoleMmaThreads, 3) k_pole_mma(PoleMmaArgs a) 
                 }
             }
             __syncthreads();
-            // the rounded limbs: limb k on warp k % 4, a lane per column, so that each limb plane is written in
-            // runs of consecutive outputs
+            // the rounded limbs: a quarter of the limbs per warp, a lane per column, so that each limb plane is
+            // written in runs of consecutive outputs
             if (lane < nn) {
                 const PmHead h = head[lane];
                 const i64 out = obase + coff_sh[lane] + i * jst;
-                if (h.mode != PmHead::kDone)
-                    for (int k = warp; k < L; k += 4) a.om[k * a.oplane + out] = (int32_t)pm_limb<L, NW>(h, accs + lane, ast, k);
+                if (h.mode != PmHead::kDone) pm_limbs<L, NW>(h, accs + lane, ast, warp, a.om + out, a.oplane);
             }
             __syncthreads();                                         // D, the limb columns and windows are reused
         }

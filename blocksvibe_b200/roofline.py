@@ -42,13 +42,15 @@ def pole_mma_geometry(L):
 
 
 def pole_mma_macs(lev, N, S, L):
-    """int8 MACs of both stages of b3d_pole_level_mma on one level: (issued by the MMAs, digit products of the
-    exact sums).  Per task and stage: S rows x S entries x U / 32 K steps x MT tiles of 128 x NC x 32 MACs per
-    column chunk; the exact sums need S^2 N (4 L)^2 digit products."""
+    """int8 MACs of both stages of b3d_pole_level_mma on one level, N = S^2 B numbers per task as in
+    pole_level_bytes: (issued by the MMAs, digit products of the exact sums).  A task has S B columns; per task
+    and stage: S rows x S entries x U / 32 K steps x MT tiles of 128 x NC x 32 MACs per column chunk; the exact
+    sums need S^2 (S B) (4 L)^2 digit products."""
     U, MT = pole_mma_geometry(L)
     T = len(lev["t_slot"])
-    nc = 32 if N >= 32 else 16 * (-(-N // 16))
-    chunks = -(-N // nc)
+    cols = N // S
+    nc = 32 if cols >= 32 else 16 * (-(-cols // 16))
+    chunks = -(-cols // nc)
     issued = 2 * T * chunks * S * S * (U // 32) * MT * 128 * nc * 32
-    useful = 2 * T * S * S * N * (4 * L) ** 2
+    useful = 2 * T * S * S * cols * (4 * L) ** 2
     return issued, useful

@@ -26,6 +26,6 @@ def test_mma_geometry_mirrors_the_kernel():
     assert RL.pole_mma_geometry(34) == (160, 2)
     assert RL.pole_mma_geometry(46) == (192, 2)
     lev = {"t_slot": [0] * 10}
-    issued, useful = RL.pole_mma_macs(lev, 30, 5, 34)
+    issued, useful = RL.pole_mma_macs(lev, 150, 5, 34)              # S^2 B = 150 numbers: 30 columns
     assert issued == 2 * 10 * 5 * 5 * 5 * 2 * 128 * 32 * 32
     assert useful == 2 * 10 * 25 * 30 * 136 ** 2
