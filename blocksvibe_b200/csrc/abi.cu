@@ -151,7 +151,7 @@ int b3d_resize(int L, const int32_t* m, const int64_t* e, int64_t plane, int64_t
 
 namespace {
 b3d::RnsTables tables_of(const b3d_rns_tables* t) {
-    return b3d::RnsTables{t->p, t->mu, t->w, t->conv, t->inv, t->mj, t->mfull, t->rp, t->np, t->ml};
+    return b3d::RnsTables{t->p, t->mu, t->w, t->conv, t->inv, t->mj, t->mfull, t->np, t->ml, t->mtop, t->msw};
 }
 }  // namespace
 

@@ -12,9 +12,9 @@
 //      (cp.async.bulk, the TMA engine) on an mbarrier, one thread issues tcgen05.mma.kind::i8 over K into a
 //      TMEM accumulator (128 lanes x TN columns, int32), and the epilogue reads TMEM with tcgen05.ld and folds
 //      the 16 digit products of each output, sum_{s,t} D[4i+s][4l+t] 2^(8(s+t)), to a residue mod p_j.
-//   3. k_rns_crt: per output, y_j = r_j (M/p_j)^-1 mod p_j, q = round(sum_j y_j / p_j) (double precision: the
-//      fraction stays within 1/4 of an integer because |P| < M/4), P = sum_j y_j (M/p_j) - q M exactly in
-//      limbs, rounded to NB bits with the exponents of its row and column.
+//   3. k_rns_crt: per output, y_j = r_j (M/p_j)^-1 mod p_j, x' = sum_j y_j (M/p_j) exactly in limbs,
+//      q = round(x' / M) from two words of x' in integers (crt_quotient: x' / M lies within 1/8 of an integer
+//      because |P| < M/8), P = x' - q M, rounded to NB bits with the exponents of its row and column.
 //
 // Every spin-wait (mbarrier phases) has an iteration limit; on expiry the CTA records an error code in a
 // device flag, waits (bounded) for its own copies, frees its TMEM and returns.
@@ -41,9 +41,28 @@ struct RnsTables {
     const uint32_t* inv;     // (np) (M / p)^-1 mod p
     const uint32_t* mj;      // (np, ML) M / p, little-endian limbs
     const uint32_t* mfull;   // (ML) M
-    const double* rp;        // (np) 1 / p
     int np, ml;
+    uint64_t mtop;           // floor(M / 2^(32 msw))
+    int msw;                 // word offset with 32 msw >= bitlen(M) - 56
 };
+
+// The CRT quotient q = round(x' / M) for x' = sum_j y_j M / p_j = P + q M with |P| < M / 8 (the prime count
+// guarantees it): from the words msw, msw + 1 of x' (x' < 128 M < 2^(32 msw + 63)) and mtop = floor(M / 2^(32 msw))
+// >= 2^23, xt / mtop is within 2^-16 of x' / M, which lies within 1/8 of q: round(xt / mtop) = q, found by seven
+// compare-and-add steps (q <= np < 128) in 64-bit integers.  No floating point.
+template <int N>
+__device__ __forceinline__ uint32_t crt_quotient(const u32 (&x)[N], int msw, uint64_t mtop) {
+    uint64_t xt = 0;
+#pragma unroll
+    for (int c = 0; c < N; c++)
+        if (c == msw) xt = ((uint64_t)(c + 1 < N ? x[c + 1] : 0u) << 32) | x[c];
+    const uint64_t num = 2 * xt + mtop, den = 2 * mtop;        // round(xt / mtop) = floor(num / den)
+    uint32_t q = 0;
+#pragma unroll
+    for (int b = 6; b >= 0; b--)
+        if ((uint64_t)(q + (1u << b)) * den <= num) q += 1u << b;
+    return q;
+}
 
 // x mod p for x < 2^62, Barrett with mu = floor(2^62 / p), 2^30 < p < 2^31
 // (the quotient estimate is at most 3 below the true quotient)
@@ -636,7 +655,7 @@ __global__ void __launch_bounds__(128, 1) k_rns_split_mma(RnsSplit a, RnsTables 
 // B = the constant matrix T[pos][4 j + a] = byte (pos - a) of M / p_j (two tiles of NH rows), so that
 // S[e][pos] = sum_{j,a} y_{j,a}(e) T[pos][4 j + a] and x' = sum_pos S[pos] 2^(8 pos) = sum_j y_j M / p_j
 // exactly (S < 4 np 255^2 < 2^25).  The epilogue thread of output e carries S into limbs, subtracts
-// round(x' / M) M (from the top limbs, in double precision) and rounds once to NB bits.
+// round(x' / M) M (crt_quotient, integers) and rounds once to NB bits.
 struct RnsCrt {
     const uint8_t* A;        // (tiles, 128 x Kc) y bytes
     const uint8_t* T;        // (2 NH x Kc) constant Toeplitz digits, tiles of NH rows
@@ -759,13 +778,7 @@ __global__ void __launch_bounds__(128, 1) k_rns_crt_mma(RnsCrt a, RnsTables tb) 
             x[c] = (uint32_t)carry;
             carry >>= 32;
         }
-        // q = round(x' / M) from the top limbs
-        double xt = 0.0, mt = 0.0;
-#pragma unroll
-        for (int c = NX - 1; c >= ML - 4; c--) xt = xt * 4294967296.0 + (double)x[c];
-#pragma unroll
-        for (int c = ML - 1; c >= ML - 4; c--) mt = mt * 4294967296.0 + (double)__ldg(tb.mfull + c);
-        const uint32_t q = (uint32_t)llrint(xt / mt);
+        const uint32_t q = crt_quotient<NX>(x, tb.msw, tb.mtop);
         uint32_t mc = 0;
         uint64_t borrow = 0;
 #pragma unroll
@@ -815,14 +828,12 @@ __global__ void k_rns_crt(const uint32_t* __restrict__ res, int64_t n, const int
     int64_t Ea = ea[b * M + row], Eb = eb[b * N + col];
     u32 acc[NA];
     zero(acc);
-    double f = 0.0;
     const int np = tb.np;
     for (int jj = 0; jj < np; jj++) {
         uint32_t r = res[(size_t)jj * n + e];
         uint32_t p = __ldg(tb.p + jj);
         uint64_t mu = __ldg(tb.mu + jj);
         uint32_t y = barrett((uint64_t)r * __ldg(tb.inv + jj), p, mu);
-        f += (double)y * __ldg(tb.rp + jj);
         // acc += y * (M / p_j)
         const uint32_t* mj = tb.mj + (size_t)jj * ML;
         uint32_t carry = 0;
@@ -834,8 +845,8 @@ __global__ void k_rns_crt(const uint32_t* __restrict__ res, int64_t n, const int
         }
         acc[ML] += carry;
     }
-    // subtract round(f) M: the result is the signed product in (-M/4, M/4)
-    uint32_t q = (uint32_t)llrint(f);
+    // subtract round(x' / M) M: the result is the signed product in (-M/8, M/8)
+    const uint32_t q = crt_quotient<NA>(acc, tb.msw, tb.mtop);
     uint32_t borrow = 0;
     {
         uint32_t carry = 0;

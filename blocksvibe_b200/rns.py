@@ -18,7 +18,7 @@ _Q = ctypes.c_int64
 
 class RnsTables(ctypes.Structure):
     _fields_ = [("p", _P), ("mu", _P), ("w", _P), ("conv", _P), ("inv", _P), ("mj", _P), ("mfull", _P),
-                ("rp", _P), ("np", _I), ("ml", _I)]
+                ("np", _I), ("ml", _I), ("mtop", ctypes.c_uint64), ("msw", _I)]
 
 
 class RnsMmaArgs(ctypes.Structure):
@@ -100,6 +100,25 @@ def layout(L):
     return np_.value, ml.value
 
 
+def crt_quotient_words(M):
+    """(msw, mtop) of the integer CRT quotient (csrc/rns.cuh crt_quotient): the least word offset with
+    32 msw >= bitlen(M) - 56, and floor(M / 2^(32 msw))"""
+    msw = max(0, -(-(M.bit_length() - 56) // 32))
+    return msw, M >> (32 * msw)
+
+
+def crt_quotient(xp, msw, mtop):
+    """the kernels' quotient: round(xt / mtop) by seven compare-and-add steps, xt = words msw, msw + 1 of x'"""
+    xt = (xp >> (32 * msw)) & ((1 << 64) - 1)
+    num, den = 2 * xt + mtop, 2 * mtop
+    assert num < 1 << 64
+    q = 0
+    for b in range(6, -1, -1):
+        if (q + (1 << b)) * den <= num:
+            q += 1 << b
+    return q
+
+
 class Tables:
     """constant tables for L-limb operands on one device"""
 
@@ -121,7 +140,7 @@ class Tables:
         self.inv = t([pow(m % p, -1, p) for m, p in zip(mj, ps)], np.uint32).view(torch.int32)
         self.mj = t([limbs(m, ml) for m in mj], np.uint32).view(torch.int32)
         self.mfull = t(limbs(M, ml), np.uint32).view(torch.int32)
-        self.rp = t([1.0 / p for p in ps], np.float64)
+        self.msw, self.mtop = crt_quotient_words(M)
         self.np, self.ml = npr, ml
         self.err = torch.zeros(1, dtype=torch.int32, device=device)
         # CRT operand geometry and the constant Toeplitz digits T[pos][4 j + a] = byte (pos - a) of M / p_j
@@ -150,7 +169,8 @@ class Tables:
                  for h in range(2)]
         self.C = torch.from_numpy(np.ascontiguousarray(np.concatenate([t.reshape(-1) for t in tiles]))).to(device)
         self.c = RnsTables(self.p.data_ptr(), self.mu.data_ptr(), self.w.data_ptr(), self.conv.data_ptr(),
-                           self.inv.data_ptr(), self.mj.data_ptr(), self.mfull.data_ptr(), self.rp.data_ptr(), npr, ml)
+                           self.inv.data_ptr(), self.mj.data_ptr(), self.mfull.data_ptr(), npr, ml, self.mtop,
+                           self.msw)
 
 
 _TABLES = {}

@@ -147,8 +147,9 @@ typedef struct b3d_rns_tables {
     const uint32_t* inv;     /* (np) (M / p)^-1 mod p */
     const uint32_t* mj;      /* (np, ml) M / p, 32-bit limbs */
     const uint32_t* mfull;   /* (ml) M */
-    const double* rp;        /* (np) 1 / p */
     int np, ml;
+    uint64_t mtop;           /* floor(M / 2^(32 msw)): the CRT quotient's integer estimate */
+    int msw;                 /* word offset: 32 msw >= bitlen(M) - 56 (so M / 2^(32 msw) >= 2^23) */
 } b3d_rns_tables;
 
 /* primes and limbs of M the kernels for L limbs expect (K <= 4096) */
