@@ -630,6 +630,30 @@ def measure_set(dev, groups, steps, warmup, world, budget_frac=0.35):
         s1.record()
         torch.cuda.synchronize()
         out[name] = max_over_ranks(s0.elapsed_time(s1) / steps, world, dev)
+    # batched passes replayed as CUDA graphs (the production form of a batched step, as in the cfg2 line): one
+    # group at a time, its graph per chunk size captured untimed, one warm-up replay, then `steps` timed replays
+    # with CUDA events; the graph and its memory pool are released before the next group (all 58 would not fit).
+    # The timed work per group equals the launched batched pass: every chunk of every task, h_inf loaded from
+    # the resident device tensors into the graph's static input.
+    graph_ms = 0.0
+    torch.cuda.empty_cache()                               # the launched arms' cached blocks: graphs use own pools
+    for op, tasks, ns, d12, chunk in prepared:
+        parts = [tasks[i:i + chunk] for i in range(0, len(tasks), chunk)]
+        steps_of = {n: DI.GraphStep(op, n, ns, d12) for n in sorted({len(q) for q in parts})}
+        for q in parts:
+            steps_of[len(q)].run(q)
+        torch.cuda.synchronize()
+        g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        g0.record()
+        for _ in range(steps):
+            for q in parts:
+                steps_of[len(q)].run(q)
+        g1.record()
+        torch.cuda.synchronize()
+        graph_ms += g0.elapsed_time(g1) / steps
+        del steps_of
+        torch.cuda.empty_cache()
+    out["batched_graph"] = max_over_ranks(graph_ms, world, dev)
     # the serving loop: all tasks submitted at once, continuous batching per operator, two workers on their own
     # streams, admission by footprint, results left on the device for the GPU JSON writer (wall clock from the
     # first submit to the last result)
@@ -656,6 +680,10 @@ def measure_set(dev, groups, steps, warmup, world, budget_frac=0.35):
             "plain": {"value": plain_rate, "unit": "tasks/s", "ms": out["plain"],
                       "what": "one task at a time, one recursion per lambda order (the reference's schedule)"},
             "batched_over_plain": out["plain"] / out["batched"],
+            "batched_graph": {"value": world * ntask / (out["batched_graph"] / 1e3), "unit": "tasks/s",
+                              "ms": out["batched_graph"],
+                              "what": "the batched passes replayed as one CUDA graph per group and chunk size"},
+            "batched_graph_over_plain": out["plain"] / out["batched_graph"],
             "serving_loop": {"value": world * ntask / serve_s, "unit": "tasks/s", "wall_s": serve_s,
                              "requests": len(reqs), "batches": len(srv.batches) - nb0,
                              "latency_ms": {"p50": serve.percentile(lat, 0.5) * 1e3,
