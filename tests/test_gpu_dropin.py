@@ -10,7 +10,7 @@ import pytest
 import torch
 
 from helpers import agreement_bits, oracle_numerators
-from blocksvibe_b200 import dropin as DI, mpf, plan as PL, structure as S
+from blocksvibe_b200 import dropin as DI, mpf, plan as PL, recursion as RC, structure as S
 from oracle import output as OO
 
 pytestmark = pytest.mark.gpu
@@ -70,13 +70,16 @@ def test_dropin_matches_oracle_chain(cuda):
     ("cfg5_1280", dict(tj12=8, tj43=8, tjmax=4, order=7, Lam=4, precision=1280, kept=5, nq=1,
                        coords=("xt", "xt_radial"), d12="6")),
 ])
-def test_worst_bits_per_config(cuda, name, args):
+@pytest.mark.parametrize("pole", ["cuda", "mma"])
+def test_worst_bits_per_config(cuda, name, args, pole, monkeypatch):
     """the drop-in bar (blocks_3d's outputs to 2^-(prec - 8)): every output agrees with the oracle chain to more
     than prec - 8 bits (relative to each polynomial's largest coefficient); the worst case is printed per
-    configuration"""
+    configuration and pole-step form (the tensor cores, or the CUDA cores)"""
+    monkeypatch.setattr(RC, "POLE", pole)
     G, tasks, M, hstr, plan = make_group(**args)
     worst = chain_worst_bits(cuda, G, tasks, M, hstr, plan)
-    print(f"\nworst-case agreement {name}: {worst:.1f} bits (precision {G.precision}, NB {32 * DI.limbs(G.precision) - 2})")
+    print(f"\nworst-case agreement {name}, pole step {pole}: {worst:.1f} bits (precision {G.precision}, "
+          f"NB {32 * DI.limbs(G.precision) - 2})")
     assert worst > G.precision - 8, worst
 
 

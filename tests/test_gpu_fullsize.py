@@ -9,6 +9,10 @@ offline (tests/golden/make_chain_golden.py on the inputs of tests/golden/chain_c
                pole shifting) on output spins 0-4: sampled residue blocks, and the xt_radial outputs of sampled
                blocks through the drop-in runner.
 
+Both cases run with each pole-step form: the tensor cores (b3d_pole_level_mma) and the CUDA cores
+(b3d_pole_level); with one right-hand side the default form choice would take the CUDA cores, so the form is
+forced here.
+
 Bars: residues relative to their (pole, spin) block > 32 L - 64 bits (the reference's recursion bar); every
 numerator polynomial and every xt_radial block relative to its largest coefficient > prec - 8 bits (the
 drop-in bar).  The worst agreement of each case is printed."""
@@ -76,11 +80,11 @@ def residue_worst(c, fix, plan, captured):
     return worst
 
 
-def run_recursion(c, fix, cuda, R=None):
+def run_recursion(c, fix, cuda, R=None, pole="auto"):
     """the slot-recycling recursion (and, with R, the moments and numerators) on the case's inputs; the sampled
     residue blocks copied out at their level"""
     plan = PL.Plan(c["tj12"], c["tj43"], c["tjmax"], c["order"], c["pp"], reuse=True)
-    rec = RC.Recursion(plan, m_table(c, plan, cuda), c["L"], device=cuda)
+    rec = RC.Recursion(plan, m_table(c, plan, cuda), c["L"], device=cuda, pole=pole)
     h1 = hinf(c, plan, cuda)
     h = mpf.MPF(h1.m.unsqueeze(-1).contiguous(), h1.e.unsqueeze(-1).contiguous())
     want = {}
@@ -103,15 +107,17 @@ def run_recursion(c, fix, cuda, R=None):
     rec.run(h, hook=hook)
     num = der.finish(h) if der is not None else None
     torch.cuda.synchronize()
+    rec.check_errors()
     captured = {k: mpf.to_mp(v) for k, v in saved.items()}
     return plan, der, num, captured, h1
 
 
-def test_cfg2_lambda0_residues_and_numerators(cuda):
+@pytest.mark.parametrize("pole", ["mma", "cuda"])
+def test_cfg2_lambda0_residues_and_numerators(cuda, pole):
     fix = load("cfg2_n0")
     c = CC.CASES["cfg2_n0"]
     R = c["Lam"] - c["n"]
-    plan, der, num, captured, _ = run_recursion(c, fix, cuda, R=R)
+    plan, der, num, captured, _ = run_recursion(c, fix, cuda, R=R, pole=pole)
     rw = residue_worst(c, fix, plan, captured)
     num = mpf.to_mp(num)                                  # (Jo, Dout, R + 1, 2, S^2, 1)
     Sm, bits = plan.Smax, fix["bits"]
@@ -128,17 +134,19 @@ def test_cfg2_lambda0_residues_and_numerators(cuda):
                 g = [num[jo, i, e, p, a * Sm + b, 0] for i in range(der.Dout)]
                 worst = min(worst, agreement_bits(g, ref))
                 count += 1
-    print(f"\ncfg2 lambda order 0: residues {rw:.1f} bits over {len(fix['residues'])} blocks (bar {32 * c['L'] - 64}); "
+    print(f"\ncfg2 lambda order 0, pole step {pole}: residues {rw:.1f} bits over {len(fix['residues'])} blocks (bar {32 * c['L'] - 64}); "
           f"numerators {worst:.1f} bits over {count} polynomials (bar {c['precision'] - 8})")
     assert count > 0
     assert rw > 32 * c["L"] - 64, rw
     assert worst > c["precision"] - 8, worst
 
 
-def test_cfg5_shape_radial_with_pole_shifting(cuda):
+@pytest.mark.parametrize("pole", ["mma", "cuda"])
+def test_cfg5_shape_radial_with_pole_shifting(cuda, pole, monkeypatch):
     fix = load("cfg5_radial")
     c = CC.CASES["cfg5_radial"]
-    plan, _, _, captured, h1 = run_recursion(c, fix, cuda)
+    monkeypatch.setattr(RC, "POLE", pole)                 # the drop-in runner's recursions too
+    plan, _, _, captured, h1 = run_recursion(c, fix, cuda, pole=pole)
     rw = residue_worst(c, fix, plan, captured)
     G = DI.Group((4, 4, 4, 4), c["tj12"], c["tj43"], c["order"], c["Lam"], c["tjmax"], c["precision"], c["kept"])
     tjs = list(range(c["tj12"] % 2, c["tjmax"] + 1, 2))
@@ -164,7 +172,7 @@ def test_cfg5_shape_radial_with_pole_shifting(cuda):
                 g = [got[jo, p, a * Smax + b, o, d] for d in range(Dmax)]
                 worst = min(worst, agreement_bits(g, ref))
                 count += 1
-    print(f"\ncfg5 shape xt_radial: residues {rw:.1f} bits over {len(fix['residues'])} blocks (bar {32 * c['L'] - 64}); "
+    print(f"\ncfg5 shape xt_radial, pole step {pole}: residues {rw:.1f} bits over {len(fix['residues'])} blocks (bar {32 * c['L'] - 64}); "
           f"xt_radial outputs {worst:.1f} bits over {count} polynomials (bar {c['precision'] - 8})")
     assert count > 0
     assert rw > 32 * c["L"] - 64, rw
