@@ -19,7 +19,8 @@ __global__ void k_cauchy_colexp(const int32_t* __restrict__ rm, const i64* __res
     i64 t = blockIdx.x * (i64)blockDim.x + threadIdx.x;
     const i64 N = lv.N;
     if (t >= lv.nb * N) return;
-    const i64 g = t / N, n = t % N;
+    i64 g, n;
+    split2(t, N, lv.nb * N, n, g);
     const i64 ncol = lv.ncol[g];
     const i64* col = lv.col + g * lv.Kc;
     i64 E = EZ;
@@ -37,7 +38,8 @@ __global__ void k_cauchy_align(const int32_t* __restrict__ rm, const i64* __rest
     i64 t = blockIdx.x * (i64)blockDim.x + threadIdx.x;
     const i64 N = lv.N;
     if (t >= lv.nb * lv.Kc * N) return;
-    const i64 n = t % N, i = (t / N) % lv.Kc, g = t / (N * lv.Kc);
+    i64 n, i, g;
+    split3(t, N, lv.Kc, lv.nb * lv.Kc * N, n, i, g);
     const i64 E = ce[g * N + n];
     u32 a[L], s[L];
     bool neg = false;
@@ -61,7 +63,8 @@ __global__ void k_cauchy_align_sm(const int32_t* __restrict__ rm, const i64* __r
     i64 t = blockIdx.x * (i64)blockDim.x + threadIdx.x;
     const i64 N = lv.N;
     if (t >= lv.nb * lv.Kc * N) return;
-    const i64 n = t % N, i = (t / N) % lv.Kc, g = t / (N * lv.Kc);
+    i64 n, i, g;
+    split3(t, N, lv.Kc, lv.nb * lv.Kc * N, n, i, g);
     const i64 E = ce[g * N + n];
     u32 a[L], s[L];
     bool neg = false;

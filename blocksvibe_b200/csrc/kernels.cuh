@@ -22,6 +22,32 @@ struct CauchyLevel {
     const i64* col;                // (nb, Kc) physical slot of each column
 };
 
+// Index splits of a flat thread index, in 32-bit arithmetic where the whole index space fits in 31 bits
+// (64-bit division is a long software sequence on the GPU; these kernels do little else per thread).
+// split2: t = q N + n;  split3: t = (g K + i) N + n.
+__device__ __forceinline__ void split2(i64 t, i64 N, i64 total, i64& n, i64& q) {
+    if (total < (i64(1) << 31)) {
+        const u32 qq = (u32)t / (u32)N;
+        n = (u32)t - qq * (u32)N;
+        q = qq;
+    } else {
+        n = t % N;
+        q = t / N;
+    }
+}
+
+__device__ __forceinline__ void split3(i64 t, i64 N, i64 K, i64 total, i64& n, i64& i, i64& g) {
+    i64 q;
+    split2(t, N, total, n, q);
+    if (total < (i64(1) << 31)) {
+        i = (u32)q % (u32)K;
+        g = (u32)q / (u32)K;
+    } else {
+        i = q % K;
+        g = q / K;
+    }
+}
+
 // ------------------------------------------------------------------------------------------------
 // Alignment: for each (batch b, row r) of a strided view X[b, r, k] (k < K), write the mantissas shifted
 // to the row's largest exponent E (truncated below it) and E.  Output element (b, r, k) goes to
@@ -493,10 +519,19 @@ __global__ void __launch_bounds__(kCauchyThreads, 4) k_cauchy4(const int32_t* __
                           const int32_t* __restrict__ hm, const i64* __restrict__ he, i64 hplane,
                           CauchyLevel lv, int32_t* __restrict__ om, i64* __restrict__ oe, i64 oplane) {
     constexpr int TB = 32 * (L + 1), ND = (TB + W - 1) / W;
+    // reciprocals floor(2^32 / v) of the divisors, built once per block: the W = 24 and W = 22 forms are only
+    // launched for plans whose divisors are below 2^8 and 2^10 (the W = 16 form divides per term)
+    constexpr int NT = W >= 24 ? 256 : (W >= 22 ? 1024 : 1);
+    __shared__ u32 inv_tab[NT];
+    if (NT > 1) {
+        for (int v = threadIdx.x; v < NT; v += blockDim.x) inv_tab[v] = v <= 1 ? 0xFFFFFFFFu : (u32)(0x100000000ull / v);
+        __syncthreads();
+    }
     i64 t = blockIdx.x * (i64)blockDim.x + threadIdx.x;
-    const i64 N = lv.N;
-    if (t >= lv.nb * lv.Mr * N) return;
-    const i64 n = t % N, r = (t / N) % lv.Mr, g = t / (N * lv.Mr);
+    const i64 N = lv.N, total = lv.nb * lv.Mr * N;
+    if (t >= total) return;
+    i64 n, r, g;
+    split3(t, N, lv.Mr, total, n, r, g);
     if (r >= lv.nrow[g]) {
         u32 z[L];
         zero(z);
@@ -524,8 +559,8 @@ __global__ void __launch_bounds__(kCauchyThreads, 4) k_cauchy4(const int32_t* __
             const int s1 = d1 == 0 ? 0 : ((n1 != (d1 < 0)) ? -1 : 1);
             const u32 v0 = d0 == 0 ? 1u : (u32)(d0 < 0 ? -d0 : d0), v1 = d1 == 0 ? 1u : (u32)(d1 < 0 ? -d1 : d1);
             // inv = floor(2^32 / d) (2^32 - 1 for d = 1): the estimate umulhi(c, inv) is the quotient or one below it
-            const u32 i0 = v0 == 1u ? 0xFFFFFFFFu : (u32)(0x100000000ull / v0);
-            const u32 i1 = v1 == 1u ? 0xFFFFFFFFu : (u32)(0x100000000ull / v1);
+            const u32 i0 = v0 < (u32)NT ? inv_tab[v0] : (v0 == 1u ? 0xFFFFFFFFu : (u32)(0x100000000ull / v0));
+            const u32 i1 = v1 < (u32)NT ? inv_tab[v1] : (v1 == 1u ? 0xFFFFFFFFu : (u32)(0x100000000ull / v1));
             u32 r0 = 0, r1 = 0;
 #pragma unroll
             for (int j = 0; j < ND; j++) {                  // digit j from the top: dividend bits [lo, lo + width)
@@ -783,7 +818,8 @@ __global__ void __launch_bounds__(kMomThreads, 3) k_moments_stage(const int32_t*
                           i64 Q, i64 N, i64 w, i64 rows, int32_t* __restrict__ ym, i64* __restrict__ ye, i64 yplane) {
     i64 t = blockIdx.x * (i64)blockDim.x + threadIdx.x;
     if (t >= Q * N) return;
-    i64 c = t % N, q = t / N;
+    i64 c, q;
+    split2(t, N, Q * N, c, q);
     i64 ix = q_slot[q] * N + c, nn = q_n[q];
     i64 out = (w * rows + q_row[q]) * N + c;
     u32 x[L], p[L];
