@@ -8,7 +8,9 @@ pm_limbs).  This file restates those formulas limb for limb and checks them agai
 package (round_mag: NB bits, half away from zero on the magnitude) on magnitudes chosen to reach the rare
 branches: carries through runs of all-ones limbs, the renormalisation, rounded values with zero low limbs
 (the two's complement negation starting above them), and negative sums.  It also restates the carry chains in
-segments of eight limbs and the header's join of their carries, against exact sums for every tile geometry."""
+segments of eight limbs and the header's join of their carries, against exact sums for every tile geometry, and
+the operand layout: the Hankel windows and reversed column digits read through the MMAs' descriptors give the
+exact dot products as byte positions."""
 import random
 
 import pytest
@@ -233,3 +235,80 @@ def test_segment_carry_join_gives_the_exact_sum(L, P0, MT):
         got = join_segments(col, carr, NW, lo, nseg)
         exact = sum(v << (32 * (lo + w)) for w, v in enumerate(V)) % (1 << (32 * NW))
         assert got == limbs(exact, NW), (L, it)
+
+
+def _geometry(L):
+    NB, D = 32 * L - 2, 4 * L
+    U = 32 * (-(-D // 32))
+
+    def p0(mt):
+        top = 8 * L - 1 - 128 * mt
+        return 0 if top <= 0 else 16 * (-(-top // 16))
+    MT = 1 if 8 * p0(1) + 17 <= NB - 160 else 2
+    return U, MT, p0(MT)
+
+
+def balanced_digits(v, L):
+    """the bytes of v + 0x8080...80 (4 L bytes), each minus 128: v = sum_u d_u 256^u, d_u in [-128, 127]"""
+    t = v + int("80" * (4 * L), 16)
+    assert 0 <= t < 1 << (32 * L)
+    return [((t >> (8 * u)) & 0xFF) - 128 for u in range(4 * L)]
+
+
+def descriptor_matrix(buf, start, lbo, sbo, rows, kbytes):
+    """the rows x kbytes int8 matrix a canonical no-swizzle K-major descriptor addresses: core matrices of 8 rows
+    x 16 bytes, (row group g, K chunk q) at start + g sbo + q lbo, row r of a core matrix at + 16 r"""
+    import numpy as np
+    m = np.zeros((rows, kbytes), dtype=np.int64)
+    for row in range(rows):
+        for k in range(kbytes):
+            m[row, k] = buf[start + (row // 8) * sbo + (k // 16) * lbo + (row % 8) * 16 + k % 16]
+    return m
+
+
+@pytest.mark.parametrize("L,S,ncols", [(10, 3, 16), (10, 2, 32), (26, 2, 16), (30, 2, 16), (34, 2, 16)])
+def test_hankel_windows_and_reversed_digits_give_the_exact_sums(L, S, ncols):
+    """one row of a task: the byte windows of the constant's digit strings (16 bytes per offset, descriptor
+    LBO 256, SBO 128) against the reversed column digits (LBO 16 NC, SBO 128) give, through the MMAs' K steps
+    and tiles, D[p, n] whose positions from P0 sum to the exact dot products (up to the dropped low part)"""
+    import numpy as np
+    U, MT, P0 = _geometry(L)
+    NB = 32 * L - 2
+    rng = random.Random(L * 7 + S)
+    c = [rng.randrange(-(1 << NB) + 1, 1 << NB) for _ in range(S)]                  # row i of the constant
+    x = [[rng.randrange(-(1 << NB) + 1, 1 << NB) for _ in range(ncols)] for _ in range(S)]   # X[j][n]
+    # the windows: padded digit string (U zero bytes first), window o (o < NWIN) = 16 bytes from byte P0 + 1 + o
+    NWIN, FAM = 128 * MT + U - 16, 16 * (128 * MT + U - 16)
+    hank = bytearray(S * FAM)
+    for j in range(S):
+        pad = [0] * U + [d & 0xFF for d in balanced_digits(c[j], L)] + [0] * (P0 + 128 * MT + U)
+        for o in range(NWIN):
+            hank[j * FAM + 16 * o: j * FAM + 16 * o + 16] = bytes(pad[P0 + 1 + o: P0 + 17 + o])
+    hank = np.frombuffer(bytes(hank), dtype=np.int8)
+    # the B operand: column n, K index j U + u' holds digit U - 1 - u' of x[j][n]
+    bop = bytearray(S * U * ncols)
+    for j in range(S):
+        for n in range(ncols):
+            d = balanced_digits(x[j][n], L) + [0] * (U - 4 * L)
+            for up in range(U):
+                kap = j * U + up
+                bop[(kap // 16) * 16 * ncols + (n // 8) * 128 + (n % 8) * 16 + kap % 16] = d[U - 1 - up] & 0xFF
+    bop = np.frombuffer(bytes(bop), dtype=np.int8)
+    D = np.zeros((128 * MT, ncols), dtype=np.int64)
+    for mt in range(MT):
+        for j in range(S):
+            for ks in range(U // 32):
+                A = descriptor_matrix(hank, j * FAM + 2048 * mt + 512 * ks, 256, 128, 128, 32)
+                B = descriptor_matrix(bop, (j * (U // 16) + 2 * ks) * 16 * ncols, 16 * ncols, 128, ncols, 32)
+                D[128 * mt:128 * mt + 128] += A @ B.T
+    assert np.abs(D).max() < 1 << 31
+    for n in range(ncols):
+        exact = sum(c[j] * x[j][n] for j in range(S))
+        got = sum(int(D[p, n]) << (8 * (P0 + p)) for p in range(128 * MT))
+        low = 0                                                         # positions below P0, exactly
+        for pp in range(P0):
+            for j in range(S):
+                dc, dx = balanced_digits(c[j], L), balanced_digits(x[j][n], L)
+                low += sum(dc[q] * dx[pp - q] for q in range(max(0, pp - 4 * L + 1), min(pp, 4 * L - 1) + 1)) << (8 * pp)
+        assert got + low == exact, (L, n)
+        assert abs(exact - got) < 1 << (8 * P0 + 17)                   # the dropped part's bound
