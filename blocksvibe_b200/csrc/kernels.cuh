@@ -1197,12 +1197,13 @@ int Launch<L>::moments_flush(const int32_t* ym, const i64* ye, i64 yplane, const
     const unsigned grid = (unsigned)((items + kFlushThreads - 1) / kFlushThreads);
 #define B3D_FLUSH(LOC, KWC, AC) do {                                                                       \
         const int smem = kFlushThreads * kFlushKC * ((LOC) + 3) * 4;     /* above 48 KB from 46 limbs: opt in */ \
-        static bool opted = false;                                                                           \
-        if (!opted) {                                                                                        \
-            const int rc = (int)cudaFuncSetAttribute(k_moments_flush<L, LOC, KWC, AC>,                      \
-                                                     cudaFuncAttributeMaxDynamicSharedMemorySize, smem);    \
-            if (rc) return rc;                                                                               \
-            opted = true;                                                                                    \
+        static unsigned long long opted = 0;                /* devices whose limit is raised */                  \
+        const unsigned long long dbit = device_bit();                                                            \
+        if (!(opted & dbit) || !dbit) {                                                                          \
+            const int rc = (int)cudaFuncSetAttribute(k_moments_flush<L, LOC, KWC, AC>,                           \
+                                                     cudaFuncAttributeMaxDynamicSharedMemorySize, smem);         \
+            if (rc) return rc;                                                                                   \
+            opted |= dbit;                                                                                       \
         }                                                                                                    \
         k_moments_flush<L, LOC, KWC, AC><<<grid, kFlushThreads, smem, st>>>(ym, ye, yplane, row_shift, m0, W, rows, N, R1, \
                                                                             nk, nkb, NN, mm, me, mplane);    \

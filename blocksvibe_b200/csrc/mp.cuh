@@ -10,6 +10,9 @@
 // instead of a runtime word index.
 #pragma once
 #include <cstdint>
+#ifdef __CUDACC__
+#include <cuda_runtime.h>
+#endif
 
 namespace b3d {
 
@@ -467,5 +470,16 @@ template <int L> B3D_HD void add_norm_col(const u32 (&a)[L], bool na, i64 ea, co
     if (!round_mag<L>(acc, T, r, er)) { *nr = false; return; }
     *nr = neg;
 }
+
+#ifdef __CUDACC__
+// The current device as a bit of a per-process mask (0 when the device is unknown or beyond 63).  Kernel
+// attributes such as a raised shared-memory limit belong to one device's context: launchers keep a mask of
+// the devices they have configured, so that a process driving several GPUs sets them on each.
+inline unsigned long long device_bit() {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 0;
+    return 1ull << dev;
+}
+#endif
 
 }  // namespace b3d

@@ -672,12 +672,13 @@ template <int L>
 static int pole_mma_stage(PoleMmaArgs a, cudaStream_t st) {
     if (a.T == 0) return 0;
     const size_t smem = PoleMmaSmem<L>::total(a.S, a.NC);
-    static bool configured = false;
-    if (!configured) {
+    static unsigned long long configured = 0;                       // devices whose limits are raised
+    const unsigned long long dbit = device_bit();
+    if (!(configured & dbit) || !dbit) {
         int rc = (int)cudaFuncSetAttribute(k_pole_mma<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
         if (!rc) rc = (int)cudaFuncSetAttribute(k_pole_mma<L>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
         if (rc) return rc;
-        configured = true;
+        configured |= dbit;
     }
     int dev = 0, sms = 0;
     int rc = (int)cudaGetDevice(&dev);

@@ -907,12 +907,13 @@ int RnsLaunch<L>::crt(const uint32_t* res, int64_t n, const int64_t* ea, const i
 
 template <int L>
 int RnsLaunch<L>::split_mma(const RnsSplit& a, const RnsTables& tb, cudaStream_t st) {
-    static bool configured = false;
+    static unsigned long long configured = 0;            // devices whose shared-memory limit is raised
+    const unsigned long long dbit = device_bit();
     const int smem = 128 * a.Ks + 2 * a.NS * a.Ks + tb.np * 512;
-    if (!configured) {
+    if (!(configured & dbit) || !dbit) {
         int rc = (int)cudaFuncSetAttribute(k_rns_split_mma<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, kRnsSmemCap);
         if (rc) return rc;
-        configured = true;
+        configured |= dbit;
     }
     if (a.nb == 0 || a.Rp == 0) return 0;
     static int sms = 0;
@@ -930,12 +931,13 @@ int RnsLaunch<L>::split_mma(const RnsSplit& a, const RnsTables& tb, cudaStream_t
 
 template <int L>
 int RnsLaunch<L>::crt_mma(const RnsCrt& a, const RnsTables& tb, cudaStream_t st) {
-    static bool configured = false;
+    static unsigned long long configured = 0;            // devices whose shared-memory limit is raised
+    const unsigned long long dbit = device_bit();
     const int smem = (128 + 2 * a.NH) * a.Kc;
-    if (!configured) {
+    if (!(configured & dbit) || !dbit) {
         int rc = (int)cudaFuncSetAttribute(k_rns_crt_mma<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, kRnsSmemCap);
         if (rc) return rc;
-        configured = true;
+        configured |= dbit;
     }
     if (a.n == 0) return 0;
     static int sms = 0;

@@ -5,15 +5,16 @@
 namespace b3d {
 
 int rns_mma_launch(const RnsMma& a, const RnsTables& tb, cudaStream_t st) {
-    static bool configured = false;
+    static unsigned long long configured = 0;            // devices whose shared-memory limits are raised
+    const unsigned long long dbit = device_bit();
     const int smem = (128 + a.TN) * a.Kp;
-    if (!configured) {
+    if (!(configured & dbit) || !dbit) {
         int rc = (int)cudaFuncSetAttribute(k_rns_mma, cudaFuncAttributeMaxDynamicSharedMemorySize, (128 + 256) * 256);
         if (rc) return rc;
         rc = (int)cudaFuncSetAttribute(k_rns_mma4, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (128 + 256) * 256 + 128 * 256);
         if (rc) return rc;
-        configured = true;
+        configured |= dbit;
     }
     const int64_t tiles_i = (4 * a.NI + 127) / 128;
     const int groups = (tb.np + kPrimesPerCta - 1) / kPrimesPerCta;
